@@ -1,0 +1,525 @@
+// ep2d_device.cuh -- sm_100a kernels of the pseudo-transient elastoplastic RVE solver.
+//
+// Device layout (one RVE): every field is a row-major array with x (i) fastest and one
+// common row pitch (a multiple of 32 elements, >= nx + 1), so the reference's arrays
+// (EffPlast2D.cu:1577-1604: n x n nodes, (n-1)^2 corners, (n+1) x n and n x (n+1)
+// faces) all index as base[j * pitch + i].  Displacements are double-buffered
+// (ping-pong) so that one launch can read the old field in its halo while writing the
+// new one; velocities are updated in place (each face reads only its own old value).
+//
+// Materials are not stored as K/G arrays: a one-byte mask per node carries
+//   M_MAT    node inside a pore by SetMaterials' test  -> K = 0.01 K0, G = 0.01 G0
+//   M_NODE   node inside a pore by ComputeStress' test -> P = tauXX = tauYY = 0
+//   M_CORNER corner (i, j) inside a pore               -> tauXY = 0
+// which reproduces K, G (EffPlast2D.cu:708-728) and the kernel masks (:77-97) exactly
+// while moving 1 byte per cell instead of 16 (K, G) plus 8 (P0, identically 0).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ep2d_types.hpp"
+
+namespace ep2d {
+
+// ---------------------------------------------------------------------------------
+// Pore tests.
+//
+// host_pore_test: SetMaterials' / ComputeEffParams' test (EffPlast2D.cu:719-720,
+// :523-524, :539-540).  The reference evaluates it on the CPU, operation by operation;
+// the *_rn intrinsics below are never contracted into fused multiply-adds, so the
+// device result is bit-identical to the host one.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool host_pore_test(double x, double y, double Lx, double Ly, double nPores,
+                                               double rad) {
+  const double ax = __dmul_rn(__dmul_rn(0.5, Lx), __dsub_rn(1.0, __ddiv_rn(1.0, nPores)));
+  const double ay = __dmul_rn(__dmul_rn(0.5, Ly), __dsub_rn(1.0, __ddiv_rn(1.0, nPores)));
+  const double sx = __ddiv_rn(Lx, nPores), sy = __ddiv_rn(Ly, nPores);
+  for (int k = 0; k < nPores; k++) {
+    for (int l = 0; l < nPores; l++) {
+      const double a = __dadd_rn(__dsub_rn(x, ax), __dmul_rn(sx, (double)k));
+      const double b = __dadd_rn(__dsub_rn(y, ay), __dmul_rn(sy, (double)l));
+      if (__dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b))) < rad) return true;
+    }
+  }
+  return false;
+}
+
+// Face / node positions of the host-side tests, exact (no contraction).
+__device__ __forceinline__ double host_pos(double h, long n_minus, long idx) {
+  // -0.5 * h * n_minus + h * idx, evaluated as the reference's host code does
+  return __dadd_rn(__dmul_rn(__dmul_rn(-0.5, h), (double)n_minus), __dmul_rn(h, (double)idx));
+}
+
+// Mask setup (north-star item d): one thread per node.
+__global__ void k_mask(Geo g, uint8_t* __restrict__ mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const long nX = g.nx, nY = g.ny;
+  const double dX = g.dX, dY = g.dY, rad = g.rad, N = g.nPores;
+  uint8_t m = 0;
+  {  // SetMaterials, EffPlast2D.cu:713-726
+    const double x = host_pos(dX, nX - 1, i);
+    const double y = host_pos(dY, nY - 1, j);
+    const double Lx = __dmul_rn(dX, (double)(nX - 1));
+    const double Ly = __dmul_rn(dY, (double)(nY - 1));
+    if (host_pore_test(x, y, Lx, Ly, N, rad)) m |= M_MAT;
+  }
+  // ComputeStress' own tests, EffPlast2D.cu:77-97, written as the reference writes them
+  // so that the CUDA compiler treats the arithmetic the same way.
+  for (int k = 0; k < N; k++) {
+    for (int l = 0; l < N; l++) {
+      if (sqrt((-0.5 * dX * (nX - 1) + dX * i - 0.5 * dX * (nX - 1) * (1.0 - 1.0 / N) + (dX * (nX - 1) / N) * k) *
+                   (-0.5 * dX * (nX - 1) + dX * i - 0.5 * dX * (nX - 1) * (1.0 - 1.0 / N) + (dX * (nX - 1) / N) * k) +
+               (-0.5 * dY * (nY - 1) + dY * j - 0.5 * dY * (nY - 1) * (1.0 - 1.0 / N) + (dY * (nY - 1) / N) * l) *
+                   (-0.5 * dY * (nY - 1) + dY * j - 0.5 * dY * (nY - 1) * (1.0 - 1.0 / N) + (dY * (nY - 1) / N) * l)) < rad) {
+        m |= M_NODE;
+      }
+      if (i < nX - 1 && j < nY - 1) {
+        if (sqrt((-0.5 * dX * (nX - 2) + dX * i - 0.5 * dX * (nX - 1) * (1.0 - 1.0 / N) + (dX * (nX - 1) / N) * k) *
+                     (-0.5 * dX * (nX - 2) + dX * i - 0.5 * dX * (nX - 1) * (1.0 - 1.0 / N) + (dX * (nX - 1) / N) * k) +
+                 (-0.5 * dY * (nY - 2) + dY * j - 0.5 * dY * (nY - 1) * (1.0 - 1.0 / N) + (dY * (nY - 1) / N) * l) *
+                     (-0.5 * dY * (nY - 2) + dY * j - 0.5 * dY * (nY - 1) * (1.0 - 1.0 / N) + (dY * (nY - 1) / N) * l)) < rad) {
+          m |= M_CORNER;
+        }
+      }
+    }
+  }
+  mask[(size_t)j * g.pitch + i] = m;
+}
+
+// ---------------------------------------------------------------------------------
+// Affine preload / load increment (EffPlast2D.cu:349-381): U += affine strain field on
+// every face, into both buffers.  The reference does this on the host; the *_rn
+// arithmetic reproduces its rounding exactly.  zero_first: step 0 starts from U = 0
+// (EffPlast2D.cu:329-333).
+// ---------------------------------------------------------------------------------
+__global__ void k_preload(Geo g, double* ux0, double* ux1, double* uy0, double* uy1, int src, double dUxdx,
+                          double dUydy, double dUxdy, int zero_first) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const long nX = g.nx, nY = g.ny;
+  const double dUydx = dUxdy;
+  const double* uxs = src ? ux1 : ux0;
+  const double* uys = src ? uy1 : uy0;
+  if (i <= nX && j < nY) {  // Ux: (nX + 1) x nY
+    const size_t q = (size_t)j * g.pitch + i;
+    const double a = __dmul_rn(host_pos(g.dX, nX, i), dUxdx);
+    const double b = __dmul_rn(host_pos(g.dY, nY - 1, j), dUxdy);
+    const double v = __dadd_rn(zero_first ? 0.0 : uxs[q], __dadd_rn(a, b));
+    ux0[q] = v;
+    ux1[q] = v;
+  }
+  if (i < nX && j <= nY) {  // Uy: nX x (nY + 1)
+    const size_t q = (size_t)j * g.pitch + i;
+    const double a = __dmul_rn(host_pos(g.dY, nY, j), dUydy);
+    const double b = __dmul_rn(host_pos(g.dX, nX - 1, i), dUydx);
+    const double v = __dadd_rn(zero_first ? 0.0 : uys[q], __dadd_rn(a, b));
+    uy0[q] = v;
+    uy1[q] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// The fused iteration kernel (north-star items a and b).
+//
+// One launch = one pseudo-time iteration of the reference's four kernels
+// ComputeStress (:37-98) -> ComputeJ2 (:100-145) -> ComputePlasticity (:147-177) ->
+// ComputeDisp (:3-35).  Each CTA owns a TX x TY block of nodes and of the faces with
+// the same (i, j); it stages the displacement halo (radius 2) and the masks in shared
+// memory, computes trial stresses on the halo region, applies the J2 radial return
+// (nodes with the averaged tauXY, corners with averaged tauXX/tauYY), and updates the
+// velocities and displacements of its own faces.  Stresses never touch HBM except on
+// RECORD launches (checkpoints and the last iteration), which also write the stress
+// fields and fold max|V| into vmax for the convergence norm (north-star item c).
+//
+// Arithmetic is written expression by expression as in the reference kernels.
+// ---------------------------------------------------------------------------------
+template <int TX, int TY>
+struct TileSmem {
+  static constexpr int UW = TX + 3, UH = TY + 3;  // Ux, Uy, mask halo tiles
+  static constexpr int SW = TX + 2, SH = TY + 2;  // node stress and corner stress tiles
+  static constexpr int FW = TX + 1, FH = TY + 1;  // return factors
+  double ux[UH][UW];
+  double uy[UH][UW];
+  double p[SH][SW];
+  double xx[SH][SW];
+  double yy[SH][SW];
+  double xy[SH][SW];
+  double fn[FH][FW];
+  double fc[FH][FW];
+  uint8_t m[UH][UW];
+};
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int TX, int TY, bool PLASTIC, bool RECORD>
+__global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
+  using S = TileSmem<TX, TY>;
+  constexpr int UW = S::UW, UH = S::UH, SW = S::SW, SH = S::SH, FW = S::FW, FH = S::FH;
+  constexpr int NT = 256;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int nx = g.nx, ny = g.ny;
+  const size_t pitch = (size_t)g.pitch;
+  const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
+  const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
+  double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
+  double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
+
+  // ---- A: stage Ux (i in [i0-1, i0+TX+1], j in [j0-2, j0+TY]),
+  //         Uy (i in [i0-2, i0+TX], j in [j0-1, j0+TY+1]) and the mask
+  //         (nodes i in [i0-2, i0+TX], j in [j0-2, j0+TY]); zero outside the domain.
+  for (int e = tid; e < UH * UW; e += NT) {
+    const int lj = e / UW, li = e - lj * UW;
+    int i = i0 - 1 + li, j = j0 - 2 + lj;
+    s.ux[lj][li] = (i >= 0 && i <= nx && j >= 0 && j < ny) ? ux[j * pitch + i] : 0.0;
+    i = i0 - 2 + li;
+    j = j0 - 1 + lj;
+    s.uy[lj][li] = (i >= 0 && i < nx && j >= 0 && j <= ny) ? uy[j * pitch + i] : 0.0;
+    j = j0 - 2 + lj;
+    s.m[lj][li] = (i >= 0 && i < nx && j >= 0 && j < ny) ? f.mask[j * pitch + i] : (uint8_t)0;
+  }
+  __syncthreads();
+
+  const double dX = g.dX, dY = g.dY;
+  // ---- B: trial stresses.  Nodes (i0-1+li, j0-1+lj) and corners (i0-2+li, j0-2+lj).
+  for (int e = tid; e < SH * SW; e += NT) {
+    const int lj = e / SW, li = e - lj * SW;
+    {
+      const int i = i0 - 1 + li, j = j0 - 1 + lj;
+      double pv = 0.0, xv = 0.0, yv = 0.0;
+      if (i >= 0 && i < nx && j >= 0 && j < ny) {
+        const double uxa = s.ux[lj + 1][li], uxb = s.ux[lj + 1][li + 1];
+        const double uya = s.uy[lj][li + 1], uyb = s.uy[lj + 1][li + 1];
+        const uint8_t m = s.m[lj + 1][li + 1];
+        const double K = (m & M_MAT) ? g.Kp : g.K0;
+        const double G = (m & M_MAT) ? g.Gp : g.G0;
+        const double divU = (uxb - uxa) / dX + (uyb - uya) / dY;
+        pv = 0.0 - K * divU;  // P0 - K divU with P0 == 0
+        xv = 2.0 * G * ((uxb - uxa) / dX - divU / 3.0);
+        yv = 2.0 * G * ((uyb - uya) / dY - divU / 3.0);
+        if (m & M_NODE) {
+          pv = 0.0;
+          xv = 0.0;
+          yv = 0.0;
+        }
+      }
+      s.p[lj][li] = pv;
+      s.xx[lj][li] = xv;
+      s.yy[lj][li] = yv;
+    }
+    {
+      const int ci = i0 - 2 + li, cj = j0 - 2 + lj;
+      double t = 0.0;
+      if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
+        const uint8_t m00 = s.m[lj][li], m10 = s.m[lj][li + 1], m01 = s.m[lj + 1][li], m11 = s.m[lj + 1][li + 1];
+        const double Gs = ((m00 & M_MAT) ? g.Gp : g.G0) + ((m10 & M_MAT) ? g.Gp : g.G0) +
+                          ((m01 & M_MAT) ? g.Gp : g.G0) + ((m11 & M_MAT) ? g.Gp : g.G0);
+        t = 0.25 * Gs * ((s.ux[lj + 1][li] - s.ux[lj][li]) / dY + (s.uy[lj][li + 1] - s.uy[lj][li]) / dX);
+        if (m00 & M_CORNER) t = 0.0;
+      }
+      s.xy[lj][li] = t;
+    }
+  }
+  __syncthreads();
+
+  // ---- C: J2 radial return (only when NL > 1, EffPlast2D.cu:392-397).
+  if (PLASTIC) {
+    const double coh = g.coh;
+    for (int e = tid; e < FH * FW; e += NT) {
+      const int lj = e / FW, li = e - lj * FW;
+      {  // node (i0-1+li, j0-1+lj): tauXYav from the 2x2 corner block (:109-135)
+        const int i = i0 - 1 + li, j = j0 - 1 + lj;
+        double fn = 1.0;
+        if (i >= 0 && i < nx && j >= 0 && j < ny) {
+          const int ci = min(max(i - 1, 0), nx - 3), cj = min(max(j - 1, 0), ny - 3);
+          const int a = ci - (i0 - 2), b = cj - (j0 - 2);
+          double tav = 0.25 * (s.xy[b][a] + s.xy[b][a + 1] + s.xy[b + 1][a] + s.xy[b + 1][a + 1]);
+          double xv = s.xx[lj][li], yv = s.yy[lj][li];
+          double J2 = sqrt(xv * xv + yv * yv + 2.0 * tav * tav);
+          if (J2 > coh) {
+            fn = coh / J2;
+            if (RECORD) {
+              xv *= fn;
+              yv *= fn;
+              tav *= fn;
+              J2 = sqrt(xv * xv + yv * yv + 2.0 * tav * tav);
+            }
+          }
+          if (RECORD && li >= 1 && lj >= 1) {
+            f.txyav[j * pitch + i] = tav;
+            f.j2[j * pitch + i] = J2;
+          }
+        }
+        s.fn[lj][li] = fn;
+      }
+      {  // corner (i0-1+li, j0-1+lj): J2XY from averaged tauXX, tauYY (:138-144)
+        const int ci = i0 - 1 + li, cj = j0 - 1 + lj;
+        double fc = 1.0;
+        if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
+          const double sx = s.xx[lj][li] + s.xx[lj][li + 1] + s.xx[lj + 1][li] + s.xx[lj + 1][li + 1];
+          const double sy = s.yy[lj][li] + s.yy[lj][li + 1] + s.yy[lj + 1][li] + s.yy[lj + 1][li + 1];
+          const double t = s.xy[lj + 1][li + 1];
+          const double J2XY = sqrt(0.0625 * sx * sx + 0.0625 * sy * sy + 2.0 * t * t);
+          if (J2XY > coh) fc = coh / J2XY;
+          if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = J2XY;
+        }
+        s.fc[lj][li] = fc;
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < FH * FW; e += NT) {
+      const int lj = e / FW, li = e - lj * FW;
+      const double fn = s.fn[lj][li];
+      s.xx[lj][li] *= fn;
+      s.yy[lj][li] *= fn;
+      s.xy[lj + 1][li + 1] *= s.fc[lj][li];
+    }
+    __syncthreads();
+  }
+
+  // ---- D: damped momentum update and U += V dt on the CTA's own faces.
+  const double dT = g.dT;
+  const double cX = 1.0 - dT * g.dampX, cY = 1.0 - dT * g.dampY;
+  const double dtr = dT / g.rho;
+  double vmx = 0.0, vmy = 0.0;
+  for (int e = tid; e < TX * TY; e += NT) {
+    const int lj = e / TX, li = e - lj * TX;
+    const int i = i0 + li, j = j0 + lj;
+    if (i >= nx || j >= ny) continue;
+    const size_t q = j * pitch + i;
+    double vx = f.vx[q];
+    if (i > 0 && j > 0 && j < ny - 1) {
+      vx = vx * cX + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj + 1][li] + s.xx[lj + 1][li + 1] - s.xx[lj + 1][li]) / dX +
+                            (s.xy[lj + 2][li + 1] - s.xy[lj + 1][li + 1]) / dY);
+      f.vx[q] = vx;
+    }
+    uxo[q] = s.ux[lj + 2][li + 1] + vx * dT;
+    double vy = f.vy[q];
+    if (i > 0 && i < nx - 1 && j > 0) {
+      vy = vy * cY + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj][li + 1] + s.yy[lj + 1][li + 1] - s.yy[lj][li + 1]) / dY +
+                            (s.xy[lj + 1][li + 2] - s.xy[lj + 1][li + 1]) / dX);
+      f.vy[q] = vy;
+    }
+    uyo[q] = s.uy[lj + 1][li + 2] + vy * dT;
+    if (i == nx - 1) {  // face column i = nx of Ux/Vx: never updated by the reference
+      const size_t q2 = j * pitch + nx;
+      uxo[q2] = s.ux[lj + 2][li + 2];
+      if (RECORD) vmx = fmax(vmx, fabs(f.vx[q2]));
+    }
+    if (j == ny - 1) {  // face row j = ny of Uy/Vy
+      const size_t q3 = (size_t)ny * pitch + i;
+      uyo[q3] = s.uy[lj + 2][li + 2];
+      if (RECORD) vmy = fmax(vmy, fabs(f.vy[q3]));
+    }
+    if (RECORD) {
+      vmx = fmax(vmx, fabs(vx));
+      vmy = fmax(vmy, fabs(vy));
+      f.p[q] = s.p[lj + 1][li + 1];
+      f.txx[q] = s.xx[lj + 1][li + 1];
+      f.tyy[q] = s.yy[lj + 1][li + 1];
+      if (i < nx - 1 && j < ny - 1) f.txy[q] = s.xy[lj + 2][li + 2];
+    }
+  }
+  if (RECORD) {
+    for (int o = 16; o > 0; o >>= 1) {
+      vmx = fmax(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
+      vmy = fmax(vmy, __shfl_xor_sync(0xffffffffu, vmy, o));
+    }
+    if ((tid & 31) == 0) {
+      atomic_max_nonneg(&f.vmax[0], vmx);
+      atomic_max_nonneg(&f.vmax[1], vmy);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// RVE averaging (EffPlast2D.cu:430-503) as a deterministic two-level reduction:
+// per-block partials in a fixed order, then one block sums the partials in order.
+// Sums: 0..3 sigma (sigma[3] stays 0 as in the reference), 4..7 sigmaPer, 8..10 epsPer.
+// ---------------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ void block_sum_into(T (&acc)[NAVG], T* out) {
+  __shared__ T red[NAVG][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NAVG; k++) {
+    T v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NAVG) {
+    T v = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += red[threadIdx.x][q];
+    out[threadIdx.x] = v;
+  }
+}
+
+// grid: one block per group of rows; block of 256 threads, x-fastest
+__global__ void k_average(Geo g, const double* __restrict__ P, const double* __restrict__ txx,
+                          const double* __restrict__ tyy, const double* __restrict__ txy,
+                          const double* __restrict__ Ux, const double* __restrict__ Uy, double nu0, int perOffsetX,
+                          int perOffsetY, int rows_per_block, double* __restrict__ partials) {
+  const long nX = g.nx, nY = g.ny;
+  const size_t pitch = (size_t)g.pitch;
+  const double dX = g.dX, dY = g.dY;
+  double acc[NAVG];
+#pragma unroll
+  for (int k = 0; k < NAVG; k++) acc[k] = 0.0;
+  const long jb = 1 + (long)blockIdx.x * rows_per_block;
+  const long je = (jb + rows_per_block < nY - 1) ? jb + rows_per_block : nY - 1;
+  for (long j = jb; j < je; j++) {
+    for (long i = 1 + threadIdx.x; i < nX - 1; i += blockDim.x) {
+      const size_t q = j * pitch + i;
+      const double pv = P[q], xv = txx[q], yv = tyy[q];
+      acc[0] += xv - pv;
+      acc[1] += yv - pv;
+      acc[2] += txy[q];
+      acc[2] += nu0 * (xv + yv - 2.0 * pv);
+      if (i > perOffsetX && i < nX - perOffsetX && j > perOffsetY && j < nY - perOffsetY) {
+        acc[4] += xv - pv;
+        acc[5] += yv - pv;
+        acc[6] += 0.25 * (txy[q - pitch - 1] + txy[q - pitch] + txy[q - 1] + txy[q]);
+        acc[7] += nu0 * (xv + yv - 2.0 * pv);
+        acc[8] += (Ux[q + 1] - Ux[q]) / dX;
+        acc[9] += (Uy[q + pitch] - Uy[q]) / dY;
+        acc[10] += 0.125 * ((Ux[q] - Ux[q - pitch]) / dY + (Uy[q] - Uy[q - 1]) / dX +
+                            (Ux[q + 1] - Ux[q - pitch + 1]) / dY + (Uy[q + 1] - Uy[q]) / dX +
+                            (Ux[q + pitch] - Ux[q]) / dY + (Uy[q + pitch] - Uy[q + pitch - 1]) / dX +
+                            (Ux[q + pitch + 1] - Ux[q + 1]) / dY + (Uy[q + pitch + 1] - Uy[q + pitch]) / dX);
+      }
+    }
+  }
+  block_sum_into<double>(acc, partials + (size_t)blockIdx.x * NAVG);
+}
+
+__global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, int width, double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= width) return;
+  double v = 0.0;
+  for (int b = 0; b < nblocks; b++) v += partials[(size_t)b * width + k];
+  out[k] = v;
+}
+
+// ---------------------------------------------------------------------------------
+// Boundary sums of getDeltaP_honest (:825-853), getDeltaP_periodic (:854-882) and
+// getTauInfty_honest (:925-942).  Element (row, col) of a flat reference index f is
+// (f / nX, f % nX), so the reference's `j * nX + nY - 1` is kept literally.
+// out: [0] dPx [1] dPy [2] dPperX [3] dPperY [4] tauX [5] tauY
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ double at_flat(const double* a, long f, long nX, size_t pitch) {
+  return a[(size_t)(f / nX) * pitch + (size_t)(f % nX)];
+}
+
+__global__ void k_boundary(Geo g, const double* __restrict__ P, const double* __restrict__ txx,
+                           const double* __restrict__ tyy, double* __restrict__ out) {
+  const long nX = g.nx, nY = g.ny;
+  const size_t pitch = (size_t)g.pitch;
+  double acc[NAVG];
+#pragma unroll
+  for (int k = 0; k < NAVG; k++) acc[k] = 0.0;
+  for (long i = 1 + threadIdx.x; i < nX - 1; i += blockDim.x) {
+    const long f0 = 0 * nX + i, f1 = (nY - 1) * nX + i;
+    const double p0 = at_flat(P, f0, nX, pitch), x0 = at_flat(txx, f0, nX, pitch), y0 = at_flat(tyy, f0, nX, pitch);
+    const double p1 = at_flat(P, f1, nX, pitch), x1 = at_flat(txx, f1, nX, pitch), y1 = at_flat(tyy, f1, nX, pitch);
+    acc[0] += x0 - p0;
+    acc[0] += y0 - p0;
+    acc[0] += x1 - p1;
+    acc[0] += y1 - p1;
+    acc[4] += x0 - y0;
+    acc[4] += x1 - y1;
+  }
+  for (long j = 1 + threadIdx.x; j < nY - 1; j += blockDim.x) {
+    const long f0 = j * nX + 0, f1 = j * nX + nY - 1;
+    const double p0 = at_flat(P, f0, nX, pitch), x0 = at_flat(txx, f0, nX, pitch), y0 = at_flat(tyy, f0, nX, pitch);
+    const double p1 = at_flat(P, f1, nX, pitch), x1 = at_flat(txx, f1, nX, pitch), y1 = at_flat(tyy, f1, nX, pitch);
+    acc[1] += x0 - p0;
+    acc[1] += y0 - p0;
+    acc[1] += x1 - p1;
+    acc[1] += y1 - p1;
+    acc[5] += x0 - y0;
+    acc[5] += x1 - y1;
+  }
+  if (g.nPores > 2) {
+    const int nP = (int)g.nPores;
+    const long r0 = nY / nP, r1 = nY * (nP - 1) / nP;
+    for (long i = nX / nP + threadIdx.x; i < nX * (nP - 1) / nP; i += blockDim.x) {
+      const long f0 = r0 * nX + i, f1 = r1 * nX + i;
+      const double p0 = at_flat(P, f0, nX, pitch), p1 = at_flat(P, f1, nX, pitch);
+      acc[2] += at_flat(txx, f0, nX, pitch) - p0;
+      acc[2] += at_flat(tyy, f0, nX, pitch) - p0;
+      acc[2] += at_flat(txx, f1, nX, pitch) - p1;
+      acc[2] += at_flat(tyy, f1, nX, pitch) - p1;
+    }
+    const long c0 = nX / nP, c1 = nX * (nP - 2) / nP;
+    for (long j = nY / nP + threadIdx.x; j < nY * (nP - 1) / g.nPores; j += blockDim.x) {
+      const long f0 = j * nX + c0, f1 = j * nX + c1;
+      const double p0 = at_flat(P, f0, nX, pitch), p1 = at_flat(P, f1, nX, pitch);
+      acc[3] += at_flat(txx, f0, nX, pitch) - p0;
+      acc[3] += at_flat(tyy, f0, nX, pitch) - p0;
+      acc[3] += at_flat(txx, f1, nX, pitch) - p1;
+      acc[3] += at_flat(tyy, f1, nX, pitch) - p1;
+    }
+  }
+  block_sum_into<double>(acc, out);
+}
+
+// Gather of the hole-edge samples (EffPlast2D.cu:552-595): idx[k] encodes field
+// (0 = Ux, 1 = Uy) in bit 62 and the reference's flat index in the low bits.
+__global__ void k_gather(Geo g, const double* __restrict__ Ux, const double* __restrict__ Uy,
+                         const unsigned long long* __restrict__ idx, int n, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const unsigned long long e = idx[k];
+  const bool isy = (e >> 62) & 1ull;
+  const unsigned long long fl = e & ((1ull << 62) - 1);
+  const unsigned long long w = isy ? (unsigned long long)g.nx : (unsigned long long)g.nx + 1;
+  const double* a = isy ? Uy : Ux;
+  out[k] = a[(fl / w) * (unsigned long long)g.pitch + fl % w];
+}
+
+// SaveAnStatic2D's numerical fields (EffPlast2D.cu:1109-1134) from the state with the
+// displacements zeroed inside the pores (EffPlast2D.cu:514-547).  Output unpadded.
+__global__ void k_static_fields(Geo g, const double* __restrict__ Ux, const double* __restrict__ Uy,
+                                const double* __restrict__ P, const double* __restrict__ txx,
+                                const double* __restrict__ tyy, const double* __restrict__ txy,
+                                double* __restrict__ unu, double* __restrict__ j1, double* __restrict__ j2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const long nX = g.nx, nY = g.ny;
+  if (i >= nX || j >= nY) return;
+  const size_t pitch = (size_t)g.pitch;
+  const double Lx = __dmul_rn(g.dX, (double)(nX - 1)), Ly = __dmul_rn(g.dY, (double)(nY - 1));
+  auto uxz = [&](long fi, long fj) {
+    return host_pore_test(host_pos(g.dX, nX, fi), host_pos(g.dY, nY - 1, fj), Lx, Ly, g.nPores, g.rad)
+               ? 0.0 : Ux[fj * pitch + fi];
+  };
+  auto uyz = [&](long fi, long fj) {
+    return host_pore_test(host_pos(g.dX, nX - 1, fi), host_pos(g.dY, nY, fj), Lx, Ly, g.nPores, g.rad)
+               ? 0.0 : Uy[fj * pitch + fi];
+  };
+  const double ux = 0.5 * (uxz(i, j) + uxz(i + 1, j));
+  const double uy = 0.5 * (uyz(i, j) + uyz(i, j + 1));
+  unu[j * nX + i] = sqrt(ux * ux + uy * uy);
+  if (i < nX - 1 && j < nY - 1) {
+    const size_t q = j * pitch + i;
+    const double Sxx = 0.25 * (-P[q] + txx[q] + -P[q + 1] + txx[q + 1] + -P[q + pitch] + txx[q + pitch] +
+                               -P[q + pitch + 1] + txx[q + pitch + 1]);
+    const double Syy = 0.25 * (-P[q] + tyy[q] + -P[q + 1] + tyy[q + 1] + -P[q + pitch] + tyy[q + pitch] +
+                               -P[q + pitch + 1] + tyy[q + pitch + 1]);
+    const double Sxy = txy[q];
+    j1[j * (nX - 1) + i] = 0.5 * (Sxx + Syy);
+    j2[j * (nX - 1) + i] = 0.5 * ((Sxx - Syy) * (Sxx - Syy) + 4.0 * Sxy * Sxy);
+  }
+}
+
+}  // namespace ep2d

@@ -1,0 +1,132 @@
+// ep2d_rve.hpp -- one RVE resident on a B200: device state, the load-step chain and
+// its records.  Shared by the single-RVE C ABI, the batched solver and the server.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ep2d.h"
+#include "ep2d_types.hpp"
+
+namespace ep2d {
+
+// thread-local last-error text (ep2d_last_error)
+void set_error(const std::string& msg);
+const char* last_error();
+int fail(int code, const std::string& msg);
+
+// RAII: make `dev` current, restore the previous device on scope exit.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev);
+  ~DeviceScope();
+};
+
+// Reference scalars derived from pa (EffPlast2D.cu:1563-1573, :1609-1611).
+struct Derived {
+  double dX, dY, dT, K0, G0, E0, nu0, rad, Y, nPores, porosity, lX, lY;
+};
+Derived derive(const ep2d_params& p);
+
+// Host-side pore test of SetMaterials / ComputeEffParams (EffPlast2D.cu:719-720).
+bool host_in_pore(const Derived& d, long nX, long nY, double x, double y);
+
+// One hole-edge sample of EffPlast2D.cu:552-595.
+struct HoleSample {
+  unsigned long long code;  // bit 62: 0 = Ux, 1 = Uy; low bits: reference flat index
+  bool zeroed;              // position inside a pore: the reference zeroes it (:514-547)
+};
+// The 20 samples per pore, in the reference's order (left, right, bottom, top).
+int hole_samples(const Derived& d, long nX, long nY, std::vector<HoleSample>* out);
+
+// Post-processing of one time step from the device sums (EffPlast2D.cu:491-696).
+// avg[NAVG]: averaging sums; bnd[NAVG]: boundary sums; samples: hole-edge values.
+void finish_record(const Derived& d, long nX, long nY, int nl, int step, const double* avg, const double* bnd,
+                   const std::vector<HoleSample>& hs, const double* samples, ep2d_step_record* r,
+                   ep2d_moduli* an, ep2d_moduli* an_per);
+
+// calc* (EffPlast2D.cu:1412-1539) from the records of the three load steps.
+void final_moduli(int nl, const ep2d_step_record& r0, const ep2d_step_record* r1, const ep2d_step_record* r2,
+                  ep2d_moduli* num, ep2d_moduli* num_per);
+
+// Validate an ep2d_params; returns EP2D_OK or an error status (with message).
+int validate_params(const ep2d_params& p);
+
+// Device row pitch (elements) for an nx-wide grid.
+int row_pitch(int nx);
+
+class Rve {
+ public:
+  Rve() = default;
+  ~Rve();
+  Rve(const Rve&) = delete;
+  Rve& operator=(const Rve&) = delete;
+
+  // allocate and initialise (constructor of the reference); stream may be null: own one
+  int create(const ep2d_params& p, cudaStream_t stream = nullptr);
+  void release();
+
+  // bytes of device memory one RVE with these parameters holds
+  static size_t footprint(const ep2d_params& p);
+
+  // ComputeEffParams (EffPlast2D.cu:311-698)
+  int solve_step(int step, double load_step_value, const double load_type[3], int n_time_steps);
+  // ComputeEffModuli without printing (EffPlast2D.cu:179-229)
+  int compute_eff_moduli(double init_load_value, const double load_type[3], int n_time_steps,
+                         ep2d_result* out);
+
+  // building blocks (used by solve_step, by the batch solver and by the tests)
+  int begin_time_step(int step, int it, double load_step_value, const double load_type[3], int n_time_steps);
+  int iterate(int64_t n, bool record_last);  // n iterations; the last one records stresses
+  int launch_one(bool record);                // one iteration kernel (no stats)
+  int reset_vmax();
+  int read_error(double* error);              // after a recording launch: D2H + error formula
+  int finish_time_step(int step, int it);     // averaging etc. into the record
+  double error_from_vmax(double vmx, double vmy) const;
+
+  int get_field(int field, double* host) const;
+  int set_field(int field, const double* host);
+  int static_fields(double* unu, double* j1, double* j2);
+
+  // state
+  ep2d_params prm{};
+  Derived d{};
+  Geo g{};
+  F64Fields f{};
+  int cur = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  // records (EffPlast2D.h:108-117)
+  int nts[EP2D_MAX_NL] = {0, 0, 0};
+  std::vector<ep2d_step_record> rec[EP2D_MAX_NL];
+  std::vector<std::vector<double>> checks[EP2D_MAX_NL];
+  double ces[3] = {0.0, 0.0, 0.0};  // curEffStrain
+  double load_type_[3] = {0.0, 0.0, 0.0};
+  bool have_step0 = false;
+  ep2d_moduli an{}, an_per{}, num{}, num_per{};
+
+  // statistics
+  double kernel_ms = 0.0;
+  int64_t launches = 0;
+  int64_t cell_updates = 0;
+
+  // device scratch
+  void* dmem = nullptr;
+  double* d_partials = nullptr;
+  double* d_out = nullptr;  // [NAVG avg][NAVG boundary][samples]
+  unsigned long long* d_idx = nullptr;
+  double* h_pin = nullptr;  // pinned mirror of d_out plus 2 vmax words
+  std::vector<HoleSample> holes;
+
+ private:
+  int run_plain(int64_t n);
+  int capture(int parity);
+  cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
+  static constexpr int kGraphLen = 64;  // iterations per captured graph (even)
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+};
+
+}  // namespace ep2d

@@ -1,0 +1,56 @@
+// ep2d_types.hpp -- plain C++ types shared by the CUDA kernels (nvcc) and the host
+// orchestration (g++), plus the kernel launch wrappers the host calls.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ep2d {
+
+enum : uint8_t { M_MAT = 1, M_NODE = 2, M_CORNER = 4 };
+
+// Per-RVE scalars, passed to kernels by value.
+struct Geo {
+  int nx, ny, pitch;
+  double dX, dY, dT, rho, dampX, dampY, coh;
+  double K0, G0, Kp, Gp;  // Kp = 0.01 * K0, Gp = 0.01 * G0 (EffPlast2D.cu:721-722)
+  double rad, nPores;
+};
+
+// Device pointers of one RVE on the FP64 path.
+struct F64Fields {
+  double* ux[2];
+  double* uy[2];
+  double* vx;
+  double* vy;
+  double *p, *txx, *tyy, *txy, *txyav, *j2, *j2xy;  // last recorded stress state
+  const uint8_t* mask;
+  unsigned long long* vmax;  // [2]: bit patterns of max|Vx|, max|Vy| (non-negative)
+};
+
+// Tile of the fused iteration kernel.
+constexpr int TILE_X = 32;
+constexpr int TILE_Y = 16;
+
+// Number of sums produced by the averaging and boundary reductions.
+constexpr int NAVG = 11;
+
+// Launch wrappers (ep2d_kernels.cu).  All are asynchronous on `stream`.
+cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream);
+cudaError_t launch_preload(const Geo& g, const F64Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
+                           int zero_first, cudaStream_t stream);
+cudaError_t launch_iter_f64(const Geo& g, const F64Fields& f, int src, bool plastic, bool record,
+                            cudaStream_t stream);
+cudaError_t prepare_kernels();  // per-device function attributes
+// averaging: writes NAVG sums to `sums` (device); `partials` holds avg_partials_len(g) doubles
+size_t avg_partials_len(const Geo& g);
+cudaError_t launch_average(const Geo& g, const F64Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,
+                           double* partials, double* sums, cudaStream_t stream);
+cudaError_t launch_boundary(const Geo& g, const F64Fields& f, double* sums, cudaStream_t stream);
+cudaError_t launch_gather(const Geo& g, const F64Fields& f, int src, const unsigned long long* idx, int n,
+                          double* out, cudaStream_t stream);
+cudaError_t launch_static_fields(const Geo& g, const F64Fields& f, int src, double* unu, double* j1, double* j2,
+                                 cudaStream_t stream);
+
+}  // namespace ep2d

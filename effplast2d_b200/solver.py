@@ -1,0 +1,182 @@
+"""ctypes binding of libep2d.so (include/ep2d.h).
+
+The library is built in-tree by effplast2d_b200.build (or __graft_entry__.build()).
+There is no fallback: without libep2d.so, or without a CUDA device, every solver call
+raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libep2d.so")
+
+_lib = None
+
+# every symbol include/ep2d.h declares
+EXPORTS = (
+    "ep2d_version", "ep2d_last_error", "ep2d_device_count", "ep2d_read_pa", "ep2d_make_pa",
+    "ep2d_field_dims", "ep2d_create", "ep2d_destroy", "ep2d_iterate", "ep2d_get_field",
+    "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
+    "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_abi_sizes", "ep2d_get_stats",
+)
+
+
+class EP2DError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("ep2d status %d: %s" % (status, message))
+        self.status = status
+
+
+def lib():
+    """Load libep2d.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libep2d.so is not built; run effplast2d_b200.build.build_lib() "
+                               "or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        vp, d, i32, i64 = ctypes.c_void_p, ctypes.c_double, ctypes.c_int32, ctypes.c_int64
+        L.ep2d_version.restype = ctypes.c_char_p
+        L.ep2d_last_error.restype = ctypes.c_char_p
+        L.ep2d_read_pa.argtypes = [ctypes.c_char_p, P(d)]
+        L.ep2d_make_pa.argtypes = [d, d, i32, i32, d, d, d, d, d, d, d, P(d)]
+        L.ep2d_field_dims.argtypes = [i32, i32, i32, P(i32), P(i32)]
+        L.ep2d_create.argtypes = [P(_abi.Params), P(vp)]
+        L.ep2d_destroy.argtypes = [vp]
+        L.ep2d_iterate.argtypes = [vp, i64]
+        L.ep2d_get_field.argtypes = [vp, i32, P(d)]
+        L.ep2d_set_field.argtypes = [vp, i32, P(d)]
+        L.ep2d_solve_step.argtypes = [vp, i32, d, P(d), i32, P(_abi.StepRecord)]
+        L.ep2d_get_record.argtypes = [vp, i32, i32, P(_abi.StepRecord)]
+        L.ep2d_get_check_errors.argtypes = [vp, i32, i32, P(d), i32, P(i32)]
+        L.ep2d_compute_eff_moduli.argtypes = [vp, d, P(d), i32, P(_abi.Result)]
+        L.ep2d_static_fields.argtypes = [vp, P(d), P(d), P(d)]
+        L.ep2d_abi_sizes.argtypes = [P(i64), i32]
+        L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64)]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise EP2DError(rc, lib().ep2d_last_error().decode(errors="replace"))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def device_count():
+    return int(lib().ep2d_device_count())
+
+
+def make_pa(lx, ly, nx, ny, k0=1.0, g0=0.5, rho0=1.0, cfl=0.5, yield_stress=1.0, porosity=0.005,
+            n_pores=1):
+    """pa.dat values (get_sigma_2D.m:3-32) computed by the library."""
+    out = np.zeros(_abi.NPARS)
+    _check(lib().ep2d_make_pa(lx, ly, nx, ny, k0, g0, rho0, cfl, yield_stress, porosity,
+                              float(n_pores), _dptr(out)))
+    return out.tolist()
+
+
+def read_pa(path):
+    out = np.zeros(_abi.NPARS)
+    _check(lib().ep2d_read_pa(os.fsencode(path), _dptr(out)))
+    return out.tolist()
+
+
+def write_pa(path, pa):
+    np.asarray(pa, dtype="<f8").tofile(path)
+
+
+class Solver:
+    """One RVE on the GPU (an ep2d_handle): the reference's EffPlast2D object."""
+
+    def __init__(self, nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000, device=0):
+        self.nx, self.ny = int(nx), int(ny)
+        self.params = _abi.make_params(nx, ny, pa, nl=nl, niter=niter, eiter=eiter,
+                                       check_every=check_every, precision=_abi.FP64, device=device)
+        h = ctypes.c_void_p()
+        _check(lib().ep2d_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ep2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def dims(self, field):
+        return _abi.field_dims(self.nx, self.ny, field)
+
+    def get(self, field):
+        w, h = self.dims(field)
+        a = np.empty((h, w), dtype=np.float64)
+        _check(lib().ep2d_get_field(self._h, _abi.FIELD_ID[field], _dptr(a)))
+        return a
+
+    def set(self, field, arr):
+        w, h = self.dims(field)
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(h, w)
+        _check(lib().ep2d_set_field(self._h, _abi.FIELD_ID[field], _dptr(a)))
+
+    def iterate(self, n):
+        _check(lib().ep2d_iterate(self._h, int(n)))
+
+    def solve_step(self, step, load_step_value, load_type, n_time_steps=1):
+        lt = np.asarray(load_type, dtype=np.float64)
+        recs = (_abi.StepRecord * n_time_steps)()
+        _check(lib().ep2d_solve_step(self._h, int(step), float(load_step_value), _dptr(lt),
+                                     int(n_time_steps), recs))
+        return [r.as_dict() for r in recs]
+
+    def record(self, step, time_step):
+        r = _abi.StepRecord()
+        _check(lib().ep2d_get_record(self._h, int(step), int(time_step), ctypes.byref(r)))
+        return r.as_dict()
+
+    def check_errors(self, step, time_step):
+        n = ctypes.c_int32()
+        _check(lib().ep2d_get_check_errors(self._h, int(step), int(time_step), None, 0, ctypes.byref(n)))
+        buf = np.zeros(max(n.value, 1))
+        _check(lib().ep2d_get_check_errors(self._h, int(step), int(time_step), _dptr(buf), n.value,
+                                           ctypes.byref(n)))
+        return buf[: n.value].tolist()
+
+    def compute_eff_moduli(self, init_load_value, load_type, n_time_steps=1):
+        lt = np.asarray(load_type, dtype=np.float64)
+        res = _abi.Result()
+        _check(lib().ep2d_compute_eff_moduli(self._h, float(init_load_value), _dptr(lt),
+                                             int(n_time_steps), ctypes.byref(res)))
+        return res.as_dict()
+
+    def static_fields(self):
+        nx, ny = self.nx, self.ny
+        unu = np.zeros((ny, nx))
+        j1 = np.zeros((ny - 1, nx - 1))
+        j2 = np.zeros((ny - 1, nx - 1))
+        _check(lib().ep2d_static_fields(self._h, _dptr(unu), _dptr(j1), _dptr(j2)))
+        return {"UnuAbs": unu, "J1nu": j1, "J2nu": j2}
+
+    def stats(self):
+        ms = ctypes.c_double()
+        la = ctypes.c_int64()
+        cu = ctypes.c_int64()
+        _check(lib().ep2d_get_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(cu)))
+        return {"kernel_ms": ms.value, "launches": la.value, "cell_updates": cu.value}

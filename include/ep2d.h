@@ -1,0 +1,201 @@
+/*
+ * ep2d.h -- C ABI of the B200-native EffPlast2D solver (libep2d.so).
+ *
+ * The reference (beacon1143/EffPlast2D) has no FFI: its boundary is the C++ class
+ * `EffPlast2D` (EffPlast2D.h:53-65) driven by `main.cu` and by the MATLAB script
+ * eff_props_2D.m through a process boundary.  Every entry point below replaces one
+ * piece of that class; the reference function it stands for is cited beside it.
+ *
+ * Conventions
+ *  - plain C types only: pointers, sizes, doubles; no CUDA or torch types;
+ *  - every function returns an int status (EP2D_OK == 0); nothing calls exit();
+ *    ep2d_last_error() returns a thread-local message for the last failure;
+ *  - fields cross the boundary in the reference's own layout: row-major, x (i)
+ *    fastest, unpadded, FP64 (EffPlast2D.cu:785-799), whatever the device layout;
+ *  - a handle owns one CUDA stream and its device buffers; handles are not
+ *    thread-safe, distinct handles may be used from distinct threads;
+ *  - a missed convergence is reported in the records (converged == 0), as the
+ *    reference's warning (EffPlast2D.cu:423-426) -- it is not an error status.
+ */
+#ifndef EP2D_H
+#define EP2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EP2D_NPARS 11   /* NPARS, EffPlast2D.h:21-23 */
+#define EP2D_MAX_NL 3   /* ComputeEffModuli supports NL <= 3, EffPlast2D.cu:182-184 */
+
+/* status codes */
+enum {
+  EP2D_OK = 0,
+  EP2D_ERR_ARG = 1,      /* invalid argument (sizes, NL, null pointers) */
+  EP2D_ERR_CUDA = 2,     /* a CUDA runtime call failed (reference: gpuErrchk, EffPlast2D.h:41-49) */
+  EP2D_ERR_IO = 3,       /* cannot open/read pa.dat (reference: ReadParams, EffPlast2D.cu:700-707) */
+  EP2D_ERR_STATE = 4,    /* call out of order (e.g. increment step before the preload) */
+  EP2D_ERR_NOMEM = 5,    /* device allocation failed or admission budget exceeded */
+  EP2D_ERR_RANGE = 6,    /* a value left the representable range of the chosen precision */
+  EP2D_ERR_NODEV = 7     /* no CUDA device, or the library was built without the kernels */
+};
+
+/* arithmetic of the pseudo-transient stencil */
+enum {
+  EP2D_FP64 = 0,         /* plain path: every field and every operation in FP64 */
+  EP2D_MIXED = 1         /* FP32 stencil bulk; FP64 residual, averages and moduli */
+};
+
+/* pa.dat layout (get_sigma_2D.m:32, read at EffPlast2D.cu:700-707, used at :1563-1573) */
+enum {
+  EP2D_PA_DX = 0, EP2D_PA_DY = 1, EP2D_PA_DT = 2, EP2D_PA_K0 = 3, EP2D_PA_G0 = 4,
+  EP2D_PA_RHO0 = 5, EP2D_PA_DAMPX = 6, EP2D_PA_DAMPY = 7, EP2D_PA_COH = 8,
+  EP2D_PA_RAD = 9, EP2D_PA_NPORES = 10
+};
+
+/* field identifiers; sizes follow the reference arrays (EffPlast2D.cu:1577-1604) */
+enum {
+  EP2D_FIELD_P = 0,      /* nx   x ny     */
+  EP2D_FIELD_TAUXX = 1,  /* nx   x ny     */
+  EP2D_FIELD_TAUYY = 2,  /* nx   x ny     */
+  EP2D_FIELD_TAUXY = 3,  /* nx-1 x ny-1   */
+  EP2D_FIELD_TAUXYAV = 4,/* nx   x ny     */
+  EP2D_FIELD_J2 = 5,     /* nx   x ny     */
+  EP2D_FIELD_J2XY = 6,   /* nx-1 x ny-1   */
+  EP2D_FIELD_UX = 7,     /* nx+1 x ny     */
+  EP2D_FIELD_UY = 8,     /* nx   x ny+1   */
+  EP2D_FIELD_VX = 9,     /* nx+1 x ny     */
+  EP2D_FIELD_VY = 10,    /* nx   x ny+1   */
+  EP2D_FIELD_K = 11,     /* nx   x ny     (materials, SetMaterials EffPlast2D.cu:708-728) */
+  EP2D_FIELD_G = 12,     /* nx   x ny     */
+  EP2D_NFIELDS = 13
+};
+
+/* Solver configuration: the reference's compile-time macros (EffPlast2D.h:17-39),
+ * its launch geometry (EffPlast2D.cu:1544-1552) and pa.dat, as run-time values. */
+typedef struct ep2d_params {
+  int32_t nx, ny;          /* grid; the reference uses nX = nY = 32*NGRID */
+  double pa[EP2D_NPARS];   /* dX,dY,dt,K0,G0,rho0,dampX,dampY,coh,rad,N */
+  int32_t nl;              /* NL: 1 elastic, 2 + bulk increment, 3 + shear increment */
+  int32_t check_every;     /* output_step (10'000, EffPlast2D.cu:1608) */
+  int64_t niter;           /* NITER */
+  double eiter;            /* EITER */
+  int32_t precision;       /* EP2D_FP64 or EP2D_MIXED */
+  int32_t device;          /* DEVICE_IDX */
+} ep2d_params;
+
+/* One time step of one load step: the per-step quantities the reference keeps in
+ * its member arrays (EffPlast2D.h:108-117) and prints (EffPlast2D.cu:311-698). */
+typedef struct ep2d_step_record {
+  int32_t step;            /* load step: 0 preload, 1 spherical increment, 2 deviatoric */
+  int32_t time_step;       /* it, 0-based */
+  int64_t iterations;      /* iterations run (iter + 1 at the break, EffPlast2D.cu:419) */
+  int32_t converged;       /* 1 if error < EITER at a checkpoint */
+  int32_t n_checks;        /* number of checkpoints evaluated */
+  double error;            /* error at the last checkpoint (EffPlast2D.cu:411-412) */
+  double macro_strain[3];  /* epsilon[step][it] == curEffStrain (EffPlast2D.cu:355-358) */
+  double sigma[4];         /* sigma[step][it]    (EffPlast2D.cu:456-494) */
+  double sigma_per[4];     /* sigmaPer[step][it] (EffPlast2D.cu:469-499) */
+  double eps_per[3];       /* epsilonPer[step][it] (EffPlast2D.cu:480-503) */
+  double delta_p;          /* getDeltaP_honest   (EffPlast2D.cu:825-853) */
+  double delta_p_per;      /* getDeltaP_periodic (EffPlast2D.cu:854-882) */
+  double tau_infty;        /* getTauInfty_honest (EffPlast2D.cu:925-942) */
+  double hole_area_pi;     /* HoleAreaPi         (EffPlast2D.cu:549-607) */
+  double internal_hole_area_pi;
+  double phi0, phi, phi_per;         /* EffPlast2D.cu:610-616 */
+  double dphi, dphi_per;             /* dPhi[step][it], dPhiPer[step][it] (:619-620) */
+  /* analytic (Yarushina) values of this step, EffPlast2D.cu:643-696; NaN when the
+   * reference does not compute them for this (NL, step) */
+  double kphi_exact_elast, kd_exact_elast;
+  double kphi_exact_plast, kd_exact_plast;
+  double kphi_exact_plast_per, kd_exact_plast_per;
+  double g_exact_elast, g_exact_plast, g_exact_plast_per;
+} ep2d_step_record;
+
+typedef struct ep2d_moduli { double kphi, kd, g; } ep2d_moduli;  /* EffModuli, EffPlast2D.h:120-134 */
+
+/* Outcome of ComputeEffModuli (EffPlast2D.cu:179-229). */
+typedef struct ep2d_result {
+  ep2d_moduli an, an_per, num, num_per;   /* eff_moduli_an, _an_per, _num, _num_per */
+  int32_t nl;
+  int32_t n_time_steps;
+  int64_t total_iterations;               /* over all load and time steps */
+  int32_t all_converged;
+  int32_t reserved;
+} ep2d_result;
+
+typedef struct ep2d_handle ep2d_handle;
+
+/* ---- library ---------------------------------------------------------------- */
+const char* ep2d_version(void);
+const char* ep2d_last_error(void);
+/* number of CUDA devices visible (0 without a GPU); never fails */
+int ep2d_device_count(void);
+
+/* ---- parameters ------------------------------------------------------------- */
+/* ReadParams (EffPlast2D.cu:700-707): read NPARS little-endian doubles from `path`. */
+int ep2d_read_pa(const char* path, double pa_out[EP2D_NPARS]);
+/* The pa.dat derivation of get_sigma_2D.m:3-32 (Lx, Ly, nx, ny, K0, G0, rho0, CFL, Y,
+ * porosity, nPores -> pa), so that callers without MATLAB produce the same file. */
+int ep2d_make_pa(double lx, double ly, int32_t nx, int32_t ny, double k0, double g0,
+                 double rho0, double cfl, double yield, double porosity, double n_pores,
+                 double pa_out[EP2D_NPARS]);
+/* width/height of a field for an nx x ny grid */
+int ep2d_field_dims(int32_t nx, int32_t ny, int32_t field, int32_t* width, int32_t* height);
+
+/* ---- single RVE --------------------------------------------------------------- */
+/* EffPlast2D::EffPlast2D (EffPlast2D.cu:1541-1612): allocate device state, build the
+ * pore/material mask on the device (SetMaterials :708-769, kernel mask :77-97),
+ * zero all fields (SetMatrixZero :785-794; P0 == 0, SetInitPressure :770-783). */
+int ep2d_create(const ep2d_params* params, ep2d_handle** out);
+/* EffPlast2D::~EffPlast2D (EffPlast2D.cu:1613-1658) */
+int ep2d_destroy(ep2d_handle* h);
+
+/* Exactly n pseudo-time iterations of the reference's kernel sequence
+ * ComputeStress -> [ComputeJ2 -> ComputePlasticity if nl > 1] -> ComputeDisp
+ * (EffPlast2D.cu:389-399), with no convergence check.  Stress-type fields
+ * (P, tau*, J2*) hold the last iteration's values afterwards. */
+int ep2d_iterate(ep2d_handle* h, int64_t n_iter);
+
+/* SaveMatrix's device->host copy (EffPlast2D.cu:795-799) / the H2D copies of
+ * EffPlast2D.cu:375,381.  Buffers are width*height doubles (ep2d_field_dims). */
+int ep2d_get_field(ep2d_handle* h, int32_t field, double* host_out);
+int ep2d_set_field(ep2d_handle* h, int32_t field, const double* host_in);
+
+/* ComputeEffParams (EffPlast2D.cu:311-698): one load step of n_time_steps time steps
+ * (affine preload, iterate to EITER with checks every check_every iterations,
+ * averaging, boundary P/tau, hole area, dPhi, analytic moduli).  `out` receives
+ * n_time_steps records (may be NULL). */
+int ep2d_solve_step(ep2d_handle* h, int32_t step, double load_step_value,
+                    const double load_type[3], int32_t n_time_steps, ep2d_step_record* out);
+/* the record of (step, time_step) kept by the handle */
+int ep2d_get_record(ep2d_handle* h, int32_t step, int32_t time_step, ep2d_step_record* out);
+/* errors evaluated at the checkpoints of (step, time_step), the values the reference
+ * prints as "Iteration k: Error is e" (EffPlast2D.cu:415-416) */
+int ep2d_get_check_errors(ep2d_handle* h, int32_t step, int32_t time_step,
+                          double* errors_out, int32_t max_n, int32_t* n_out);
+
+/* ComputeEffModuli (EffPlast2D.cu:179-229) without the printing and file output:
+ * step 0 preload, then the spherical (NL >= 2) and deviatoric (NL == 3) increments
+ * of incPercent = 0.005 (EffPlast2D.h:105), then calc* (EffPlast2D.cu:1412-1539). */
+int ep2d_compute_eff_moduli(ep2d_handle* h, double init_load_value, const double load_type[3],
+                            int32_t n_time_steps, ep2d_result* out);
+
+/* SaveAnStatic2D's numerical fields (EffPlast2D.cu:1098-1134): |u| at nodes (nx*ny),
+ * J1 and J2 at corners ((nx-1)*(ny-1)), from the state after the last load step with
+ * displacements zeroed inside the pores (EffPlast2D.cu:514-547). */
+int ep2d_static_fields(ep2d_handle* h, double* unu_abs, double* j1nu, double* j2nu);
+
+/* sizeof(ep2d_params), sizeof(ep2d_step_record), sizeof(ep2d_moduli), sizeof(ep2d_result)
+ * into out[0..n); returns the number of structs (4).  Lets a binding check its layout. */
+int ep2d_abi_sizes(int64_t* out, int32_t n);
+
+/* device time spent in the iteration kernels of this handle so far (ms), and the
+ * number of kernel launches issued for them */
+int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t* cell_updates);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EP2D_H */

@@ -1,0 +1,50 @@
+/*
+ * ep2d_oracle.h -- CPU oracle for the EffPlast2D pseudo-transient solver.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference's FP64
+ * algorithm (beacon1143/EffPlast2D, EffPlast2D.cu) used as the checker by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  The product
+ * (effplast2d_b200, libep2d.so) never links or calls it.
+ *
+ * The API mirrors include/ep2d.h one to one (orc_* <-> ep2d_*) so that a test can
+ * drive both with the same inputs and compare fields and records.
+ */
+#ifndef EP2D_ORACLE_H
+#define EP2D_ORACLE_H
+
+#include "../include/ep2d.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_state orc_state;
+
+int orc_create(const ep2d_params* params, orc_state** out);
+int orc_destroy(orc_state* s);
+int orc_set_threads(int n);
+int orc_iterate(orc_state* s, int64_t n_iter);
+int orc_get_field(orc_state* s, int32_t field, double* out);
+int orc_set_field(orc_state* s, int32_t field, const double* in);
+int orc_solve_step(orc_state* s, int32_t step, double load_step_value, const double load_type[3],
+                   int32_t n_time_steps, ep2d_step_record* out);
+int orc_get_record(orc_state* s, int32_t step, int32_t time_step, ep2d_step_record* out);
+int orc_get_check_errors(orc_state* s, int32_t step, int32_t time_step, double* errors_out,
+                         int32_t max_n, int32_t* n_out);
+int orc_compute_eff_moduli(orc_state* s, double init_load_value, const double load_type[3],
+                           int32_t n_time_steps, ep2d_result* out);
+/* SaveAnStatic2D (EffPlast2D.cu:1060-1292).  Numerical fields always; the analytic
+ * fields and error maps are written only when nPores == 1 (pointers may be NULL
+ * otherwise).  stats[6] = Uabs max, avg, J1 max, avg, J2 max, avg (NaN if N != 1). */
+int orc_static_fields(orc_state* s, double delta_p, double tau_infty,
+                      double* unu_abs, double* j1nu, double* j2nu,
+                      double* uan_abs, double* error_uabs, double* j1an, double* j2an,
+                      double* error_j1, double* error_j2, double stats[6]);
+/* kernel-level pore masks as evaluated by ComputeStress (EffPlast2D.cu:77-97):
+ * node mask nx*ny and corner mask (nx-1)*(ny-1), 1 = inside a pore */
+int orc_get_masks(orc_state* s, uint8_t* node_mask, uint8_t* corner_mask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
