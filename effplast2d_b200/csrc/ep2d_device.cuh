@@ -416,7 +416,10 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks,
 // (f / nX, f % nX), so the reference's `j * nX + nY - 1` is kept literally.
 // out: [0] dPx [1] dPy [2] dPperX [3] dPperY [4] tauX [5] tauY
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ double at_flat(const double* a, long f, long nX, size_t pitch) {
+// For ny > 2 nx the reference's `j * nX + nY - 1` runs past its array (undefined
+// behaviour there); such reads count as 0 here.
+__device__ __forceinline__ double at_flat(const double* a, long f, long nX, long nY, size_t pitch) {
+  if (f < 0 || f >= nX * nY) return 0.0;
   return a[(size_t)(f / nX) * pitch + (size_t)(f % nX)];
 }
 
@@ -429,8 +432,8 @@ __global__ void k_boundary(Geo g, const double* __restrict__ P, const double* __
   for (int k = 0; k < NAVG; k++) acc[k] = 0.0;
   for (long i = 1 + threadIdx.x; i < nX - 1; i += blockDim.x) {
     const long f0 = 0 * nX + i, f1 = (nY - 1) * nX + i;
-    const double p0 = at_flat(P, f0, nX, pitch), x0 = at_flat(txx, f0, nX, pitch), y0 = at_flat(tyy, f0, nX, pitch);
-    const double p1 = at_flat(P, f1, nX, pitch), x1 = at_flat(txx, f1, nX, pitch), y1 = at_flat(tyy, f1, nX, pitch);
+    const double p0 = at_flat(P, f0, nX, nY, pitch), x0 = at_flat(txx, f0, nX, nY, pitch), y0 = at_flat(tyy, f0, nX, nY, pitch);
+    const double p1 = at_flat(P, f1, nX, nY, pitch), x1 = at_flat(txx, f1, nX, nY, pitch), y1 = at_flat(tyy, f1, nX, nY, pitch);
     acc[0] += x0 - p0;
     acc[0] += y0 - p0;
     acc[0] += x1 - p1;
@@ -440,8 +443,8 @@ __global__ void k_boundary(Geo g, const double* __restrict__ P, const double* __
   }
   for (long j = 1 + threadIdx.x; j < nY - 1; j += blockDim.x) {
     const long f0 = j * nX + 0, f1 = j * nX + nY - 1;
-    const double p0 = at_flat(P, f0, nX, pitch), x0 = at_flat(txx, f0, nX, pitch), y0 = at_flat(tyy, f0, nX, pitch);
-    const double p1 = at_flat(P, f1, nX, pitch), x1 = at_flat(txx, f1, nX, pitch), y1 = at_flat(tyy, f1, nX, pitch);
+    const double p0 = at_flat(P, f0, nX, nY, pitch), x0 = at_flat(txx, f0, nX, nY, pitch), y0 = at_flat(tyy, f0, nX, nY, pitch);
+    const double p1 = at_flat(P, f1, nX, nY, pitch), x1 = at_flat(txx, f1, nX, nY, pitch), y1 = at_flat(tyy, f1, nX, nY, pitch);
     acc[1] += x0 - p0;
     acc[1] += y0 - p0;
     acc[1] += x1 - p1;
@@ -454,20 +457,20 @@ __global__ void k_boundary(Geo g, const double* __restrict__ P, const double* __
     const long r0 = nY / nP, r1 = nY * (nP - 1) / nP;
     for (long i = nX / nP + threadIdx.x; i < nX * (nP - 1) / nP; i += blockDim.x) {
       const long f0 = r0 * nX + i, f1 = r1 * nX + i;
-      const double p0 = at_flat(P, f0, nX, pitch), p1 = at_flat(P, f1, nX, pitch);
-      acc[2] += at_flat(txx, f0, nX, pitch) - p0;
-      acc[2] += at_flat(tyy, f0, nX, pitch) - p0;
-      acc[2] += at_flat(txx, f1, nX, pitch) - p1;
-      acc[2] += at_flat(tyy, f1, nX, pitch) - p1;
+      const double p0 = at_flat(P, f0, nX, nY, pitch), p1 = at_flat(P, f1, nX, nY, pitch);
+      acc[2] += at_flat(txx, f0, nX, nY, pitch) - p0;
+      acc[2] += at_flat(tyy, f0, nX, nY, pitch) - p0;
+      acc[2] += at_flat(txx, f1, nX, nY, pitch) - p1;
+      acc[2] += at_flat(tyy, f1, nX, nY, pitch) - p1;
     }
     const long c0 = nX / nP, c1 = nX * (nP - 2) / nP;
     for (long j = nY / nP + threadIdx.x; j < nY * (nP - 1) / g.nPores; j += blockDim.x) {
       const long f0 = j * nX + c0, f1 = j * nX + c1;
-      const double p0 = at_flat(P, f0, nX, pitch), p1 = at_flat(P, f1, nX, pitch);
-      acc[3] += at_flat(txx, f0, nX, pitch) - p0;
-      acc[3] += at_flat(tyy, f0, nX, pitch) - p0;
-      acc[3] += at_flat(txx, f1, nX, pitch) - p1;
-      acc[3] += at_flat(tyy, f1, nX, pitch) - p1;
+      const double p0 = at_flat(P, f0, nX, nY, pitch), p1 = at_flat(P, f1, nX, nY, pitch);
+      acc[3] += at_flat(txx, f0, nX, nY, pitch) - p0;
+      acc[3] += at_flat(tyy, f0, nX, nY, pitch) - p0;
+      acc[3] += at_flat(txx, f1, nX, nY, pitch) - p1;
+      acc[3] += at_flat(tyy, f1, nX, nY, pitch) - p1;
     }
   }
   block_sum_into<double>(acc, out);
