@@ -170,6 +170,14 @@ int ep2d_static_fields(ep2d_handle* h, double* unu_abs, double* j1nu, double* j2
   EP2D_GUARD({ return h->rve.static_fields(unu_abs, j1nu, j2nu); })
 }
 
+int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, double* uan_abs, double* error_uabs,
+                         double* j1an, double* j2an, double* error_j1, double* error_j2, double stats[6]) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  EP2D_GUARD({
+    return h->rve.analytic_fields(delta_p, tau_infty, uan_abs, error_uabs, j1an, j2an, error_j1, error_j2, stats);
+  })
+}
+
 int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t* cell_updates) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
   if (kernel_ms) *kernel_ms = h->rve.kernel_ms;

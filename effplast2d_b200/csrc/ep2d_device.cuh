@@ -525,4 +525,212 @@ __global__ void k_static_fields(Geo g, const double* __restrict__ Ux, const doub
   }
 }
 
+
+// ---------------------------------------------------------------------------------
+// Analytic static solution and error maps (SaveAnStatic2D, EffPlast2D.cu:1060-1292;
+// getAnalytic* :989-1059).  Complex FP64 on the device.  The complex helpers follow the
+// textbook definitions: product and quotient componentwise (quotient by Smith's
+// method), log z = (log|z|, atan2), exp z = e^re (cos, sin), and the principal square
+// root by the half-angle formulas; CUDA's real math functions do the rest.  Zone tests
+// and positions use the non-contracting *_rn arithmetic so that every node falls in
+// the same zone as in the reference's host evaluation.
+// ---------------------------------------------------------------------------------
+struct cplx {
+  double re, im;
+};
+__device__ __forceinline__ cplx c_mk(double r, double i) { return cplx{r, i}; }
+__device__ __forceinline__ cplx c_add(cplx a, cplx b) { return cplx{a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx c_sub(cplx a, cplx b) { return cplx{a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ cplx c_addr(cplx a, double r) { return cplx{a.re + r, a.im}; }  // complex + real
+__device__ __forceinline__ cplx c_rsub(double r, cplx a) { return cplx{r - a.re, 0.0 - a.im}; }  // real - complex
+__device__ __forceinline__ cplx c_radd(double r, cplx a) { return cplx{r + a.re, a.im}; }  // real + complex
+__device__ __forceinline__ cplx c_scale(double s, cplx a) { return cplx{s * a.re, s * a.im}; }
+__device__ __forceinline__ cplx c_divr(cplx a, double s) { return cplx{a.re / s, a.im / s}; }
+__device__ __forceinline__ cplx c_conj(cplx a) { return cplx{a.re, -a.im}; }
+__device__ __forceinline__ cplx c_mul(cplx a, cplx b) {
+  return cplx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ cplx c_div(cplx a, cplx b) {  // Smith (1962)
+  if (fabs(b.re) >= fabs(b.im)) {
+    const double r = b.im / b.re, den = b.re + b.im * r;
+    return cplx{(a.re + a.im * r) / den, (a.im - a.re * r) / den};
+  }
+  const double r = b.re / b.im, den = b.re * r + b.im;
+  return cplx{(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+}
+__device__ __forceinline__ cplx c_rdiv(double s, cplx b) { return c_div(cplx{s, 0.0}, b); }
+__device__ __forceinline__ double c_abs(cplx a) { return hypot(a.re, a.im); }
+__device__ __forceinline__ double c_arg(cplx a) { return atan2(a.im, a.re); }
+__device__ __forceinline__ cplx c_log(cplx a) { return cplx{log(c_abs(a)), c_arg(a)}; }
+__device__ __forceinline__ cplx c_exp(cplx a) {
+  double s, c;
+  sincos(a.im, &s, &c);
+  const double e = exp(a.re);
+  return cplx{e * c, e * s};
+}
+__device__ __forceinline__ cplx c_sqrt(cplx a) {  // principal branch, half-angle formulas
+  if (a.re == 0.0 && a.im == 0.0) return cplx{0.0, a.im};
+  const double m = c_abs(a);
+  if (a.re >= 0.0) {
+    const double t = sqrt(0.5 * (m + a.re));
+    return cplx{t, a.im / (2.0 * t)};
+  }
+  const double t = sqrt(0.5 * (m - a.re));
+  return cplx{fabs(a.im) / (2.0 * t), copysign(t, a.im)};
+}
+
+struct AnalyticCore {
+  cplx zeta, w, dw, wv, Phi, Psi;
+};
+
+// getAnalytic, EffPlast2D.cu:989-1012
+__device__ AnalyticCore an_core(const AnParams& a, double x, double y) {
+  AnalyticCore o;
+  const cplx z = c_mk(x, y);
+  double signx = x > 0.0 ? 1.0 : -1.0;
+  if (fabs(x) < 2.220446049250313e-16) signx = 1.0;
+  o.zeta = c_divr(c_divr(c_add(z, c_scale(signx, c_sqrt(c_addr(c_mul(z, z), 4.0 * a.c0 * a.c0 * a.kappa)))), 2.0), a.c0);
+  o.w = c_scale(a.c0, c_sub(o.zeta, c_rdiv(a.kappa, o.zeta)));
+  o.dw = c_scale(a.c0, c_radd(1.0, c_rdiv(a.kappa, c_mul(o.zeta, o.zeta))));
+  o.wv = c_scale(a.c0, c_sub(c_rdiv(1.0, o.zeta), c_scale(a.kappa, o.zeta)));
+  o.Phi = c_rsub(-a.Y * a.xi / 2.0, c_scale(a.Y * a.xi, c_log(c_divr(c_div(o.w, o.zeta), a.rad))));
+  o.Psi = c_div(c_mul(c_rdiv(-a.Y * a.xi, o.zeta), o.wv), o.dw);
+  return o;
+}
+
+// getAnalyticUelast, EffPlast2D.cu:1014-1026
+__device__ double an_u_elast_abs(const AnParams& a, double x, double y) {
+  const AnalyticCore o = an_core(a, x, y);
+  const cplx lg = c_log(c_divr(c_div(o.w, o.zeta), a.rad));
+  const cplx phi = c_sub(c_mul(c_scale(-a.Y * a.xi, o.w), c_addr(lg, 0.5)), c_rdiv(2.0 * a.c0 * a.tauInfty, o.zeta));
+  const cplx psi = c_scale(a.c0 * a.Y * a.xi, c_add(c_rdiv(1.0, o.zeta), c_scale(a.kappa, o.zeta)));
+  const cplx dphi = c_mul(o.Phi, o.dw);
+  const double k = 1.0 + 6.0 * a.G0 / (a.G0 + 3.0 * a.K0);
+  const cplx U = c_divr(c_divr(c_sub(c_sub(c_scale(k, phi), c_mul(c_div(o.w, c_conj(o.dw)), c_conj(dphi))), c_conj(psi)), 2.0),
+                        a.G0);
+  return c_abs(U);
+}
+
+// getAnalyticUrHydro, EffPlast2D.cu:1027-1029
+__device__ __forceinline__ double an_ur_hydro(const AnParams& a, double r) {
+  return -0.5 * a.Y * a.rad * a.rad * exp((a.deltaP - a.Y) / a.Y) / (a.G0 * r);
+}
+
+// getAnalyticJelast, EffPlast2D.cu:1036-1051
+__device__ void an_j_elast(const AnParams& a, double x, double y, double* J1, double* J2) {
+  const AnalyticCore o = an_core(a, x, y);
+  const cplx z = c_mk(x, y);
+  const cplx dPhi = c_div(c_rdiv(-2.0 * a.xi * a.Y * a.kappa, o.zeta), c_addr(c_mul(o.zeta, o.zeta), -a.kappa));
+  const double ang = -2.0 * c_arg(z);
+  const cplx e = c_exp(c_mk(ang * 0.0, ang * 1.0));
+  const cplx F = c_div(c_scale(2.0, c_add(c_mul(c_div(c_conj(o.w), o.dw), dPhi), o.Psi)), e);
+  const double Srr = 2.0 * o.Phi.re - F.re / 2.0;
+  const double Sff = 2.0 * o.Phi.re + F.re / 2.0;
+  const double Srf = F.im / 2.0;
+  *J1 = 0.5 * (Srr + Sff);
+  *J2 = 0.5 * ((Srr - Sff) * (Srr - Sff) + 4.0 * Srf * Srf);
+}
+
+__device__ __forceinline__ double sq_rn(double v) { return __dmul_rn(v, v); }
+
+// One thread per node; stats[blockIdx][8] = Umax, Usum, Un, J1max, J1sum, J2max, J2sum, Jn
+__global__ void k_analytic(Geo g, AnParams a, const double* __restrict__ unu, const double* __restrict__ j1nu,
+                           const double* __restrict__ j2nu, double* __restrict__ uan, double* __restrict__ eu,
+                           double* __restrict__ j1an, double* __restrict__ j2an, double* __restrict__ ej1,
+                           double* __restrict__ ej2, double* __restrict__ stats) {
+  const long nX = g.nx, nY = g.ny;
+  double st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const long total = nX * nY;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long j = e / nX, i = e - j * nX;
+    const long q = j * nX + i;
+    const double x = host_pos(g.dX, nX - 1, i), y = host_pos(g.dY, nY - 1, j);
+    const double r2 = __dadd_rn(sq_rn(x), sq_rn(y));
+    const double r = __dsqrt_rn(r2);
+    double ua;
+    if (__dadd_rn(__ddiv_rn(sq_rn(x), sq_rn(a.Rx)), __ddiv_rn(sq_rn(y), sq_rn(a.Ry))) > 1.0) {
+      ua = a.hydro ? fabs(an_ur_hydro(a, r)) : an_u_elast_abs(a, x, y);
+    } else if (__dadd_rn(__ddiv_rn(sq_rn(x), sq_rn(a.rx)), __ddiv_rn(sq_rn(y), sq_rn(a.ry))) > 1.0) {
+      ua = fabs(an_ur_hydro(a, r));
+    } else {
+      ua = 0.0;
+    }
+    uan[q] = ua;
+    double err = 0.0;
+    const double un = unu[q];
+    if (r2 > sq_rn(a.Rmin) && r2 < sq_rn(a.Rmax) && fabs(un) > a.eps) {
+      err = fabs((ua - un) / ua);
+      st[0] = fmax(st[0], err);
+      st[1] += err;
+      st[2] += 1.0;
+      if (fabs(err) > 0.5) err = -0.5;
+    }
+    eu[q] = err;
+    if (i < nX - 1 && j < nY - 1) {
+      const long c = j * (nX - 1) + i;
+      const double xs = __dadd_rn(x, __dmul_rn(0.5, g.dX)), ys = __dadd_rn(y, __dmul_rn(0.5, g.dY));
+      const double rs2 = __dadd_rn(sq_rn(xs), sq_rn(ys));
+      const double rs = __dsqrt_rn(rs2);
+      double J1 = 0.0, J2 = 0.0;
+      if (__dadd_rn(__ddiv_rn(sq_rn(xs), sq_rn(a.Rx)), __ddiv_rn(sq_rn(ys), sq_rn(a.Ry))) > 1.0) {
+        if (a.hydro) {
+          const double relR = a.rad / rs;
+          const double Srr = -a.deltaP + relR * relR * a.Y * exp(a.deltaP / a.Y - 1);
+          const double Sff = -a.deltaP - relR * relR * a.Y * exp(a.deltaP / a.Y - 1);
+          J1 = 0.5 * (Srr + Sff);
+          J2 = 0.5 * ((Srr - Sff) * (Srr - Sff));
+        } else {
+          an_j_elast(a, xs, ys, &J1, &J2);
+        }
+      } else if (__dadd_rn(__ddiv_rn(sq_rn(xs), sq_rn(a.rx)), __ddiv_rn(sq_rn(ys), sq_rn(a.ry))) > 1.0) {
+        const double Srr = -2.0 * a.xi * a.Y * log(rs / a.rad);
+        const double Sff = -2.0 * a.xi * a.Y * (1.0 + log(rs / a.rad));
+        J1 = 0.5 * (Srr + Sff);
+        J2 = 0.5 * ((Srr - Sff) * (Srr - Sff));
+      }
+      j1an[c] = J1;
+      j2an[c] = J2;
+      double e1 = 0.0, e2 = 0.0;
+      if (rs2 > sq_rn(a.Rmin) && rs2 < sq_rn(a.Rmax)) {
+        if (fabs(j1nu[c]) > a.eps) {
+          e1 = fabs((J1 - j1nu[c]) / J1);
+          st[3] = fmax(st[3], e1);
+          st[4] += e1;
+          if (fabs(e1) > 0.5) e1 = -0.5;
+        }
+        if (fabs(j2nu[c]) > a.eps) {
+          e2 = fabs((J2 - j2nu[c]) / J2);
+          st[5] = fmax(st[5], e2);
+          st[6] += e2;
+          if (fabs(e2) > 0.5) e2 = -0.5;
+        }
+        st[7] += 1.0;
+      }
+      ej1[c] = e1;
+      ej2[c] = e2;
+    }
+  }
+  // block reduction: max for 0, 3, 5; sums for the rest
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double v = st[k];
+    const bool mx = (k == 0 || k == 3 || k == 5);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_down_sync(0xffffffffu, v, o);
+      v = mx ? fmax(v, u) : v + u;
+    }
+    if (lane == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int k = threadIdx.x;
+    const bool mx = (k == 0 || k == 3 || k == 5);
+    double v = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) v = mx ? fmax(v, red[k][q]) : v + red[k][q];
+    stats[(size_t)blockIdx.x * 8 + k] = v;
+  }
+}
+
 }  // namespace ep2d

@@ -94,4 +94,11 @@ cudaError_t launch_static_fields(const Geo& g, const F64Fields& f, int src, doub
   return cudaGetLastError();
 }
 
+cudaError_t launch_analytic(const Geo& g, const AnParams& a, const double* unu, const double* j1nu, const double* j2nu,
+                            double* uan, double* eu, double* j1an, double* j2an, double* ej1, double* ej2,
+                            double* stats, cudaStream_t stream) {
+  k_analytic<<<ANALYTIC_BLOCKS, 256, 0, stream>>>(g, a, unu, j1nu, j2nu, uan, eu, j1an, j2an, ej1, ej2, stats);
+  return cudaGetLastError();
+}
+
 }  // namespace ep2d

@@ -3,8 +3,10 @@
 // reference's host code, which nvcc hands to the same compiler with default flags).
 #include "ep2d_rve.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <set>
 
@@ -724,6 +726,80 @@ int Rve::static_fields(double* unu, double* j1, double* j2) {
   cudaError_t se = cudaStreamSynchronize(stream);
   if (e != cudaSuccess || se != cudaSuccess)
     return fail(EP2D_ERR_CUDA, std::string("static fields: ") + cudaGetErrorString(e != cudaSuccess ? e : se));
+  return EP2D_OK;
+}
+
+int Rve::analytic_fields(double deltaP, double tauInfty, double* uan, double* eu, double* j1an, double* j2an,
+                         double* ej1, double* ej2, double stats[6]) {
+  if (!uan || !eu || !j1an || !j2an || !ej1 || !ej2 || !stats) return fail(EP2D_ERR_ARG, "null output buffer");
+  DeviceScope ds(device);
+  // scalars, EffPlast2D.cu:1062-1078, in host arithmetic
+  AnParams a{};
+  a.deltaP = deltaP;
+  a.tauInfty = tauInfty;
+  a.Y = d.Y;
+  a.rad = d.rad;
+  a.G0 = d.G0;
+  a.K0 = d.K0;
+  a.hydro = (std::abs(load_type_[0] - load_type_[1]) < std::numeric_limits<double>::epsilon()) &&
+            std::abs(load_type_[2]) < std::numeric_limits<double>::epsilon();
+  a.Rmin = d.rad;
+  a.Rmax = 0.5 * d.dX * (prm.nx - 1) - d.dX * 20.0;
+  a.eps = 1.0e-18;
+  a.xi = (deltaP > 0.0) ? 1.0 : -1.0;
+  a.kappa = tauInfty / d.Y * a.xi;
+  a.c0 = d.rad * std::exp(std::abs(deltaP) / 2.0 / d.Y - 0.5);
+  a.rx = d.rad + (-0.5 * d.Y * d.rad * d.rad * std::exp((deltaP - d.Y) / d.Y) / (d.G0 * d.rad));
+  a.ry = a.rx;
+  a.Rx = a.c0 * (1.0 - a.kappa);
+  a.Ry = a.c0 * (1.0 + a.kappa);
+  const size_t nn = (size_t)prm.nx * prm.ny, nc = (size_t)(prm.nx - 1) * (prm.ny - 1);
+  const size_t nst = (size_t)ANALYTIC_BLOCKS * 8;
+  double* tmp = nullptr;
+  EP2D_CK(cudaMallocAsync(&tmp, (3 * nn + 6 * nc + nst) * sizeof(double), stream));
+  double* unu = tmp;
+  double* j1nu = unu + nn;
+  double* j2nu = j1nu + nc;
+  double* d_uan = j2nu + nc;
+  double* d_eu = d_uan + nn;
+  double* d_j1 = d_eu + nn;
+  double* d_j2 = d_j1 + nc;
+  double* d_e1 = d_j2 + nc;
+  double* d_e2 = d_e1 + nc;
+  double* d_st = d_e2 + nc;
+  std::vector<double> st(nst);
+  cudaError_t e = launch_static_fields(g, f, cur, unu, j1nu, j2nu, stream);
+  if (e == cudaSuccess) e = launch_analytic(g, a, unu, j1nu, j2nu, d_uan, d_eu, d_j1, d_j2, d_e1, d_e2, d_st, stream);
+  struct {
+    double* h;
+    const double* dd;
+    size_t n;
+  } cp[] = {{uan, d_uan, nn}, {eu, d_eu, nn}, {j1an, d_j1, nc}, {j2an, d_j2, nc}, {ej1, d_e1, nc}, {ej2, d_e2, nc},
+            {st.data(), d_st, nst}};
+  for (auto& c : cp)
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.h, c.dd, c.n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+  cudaFreeAsync(tmp, stream);
+  cudaError_t se = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess || se != cudaSuccess)
+    return fail(EP2D_ERR_CUDA, std::string("analytic fields: ") + cudaGetErrorString(e != cudaSuccess ? e : se));
+  double umax = 0, usum = 0, un = 0, j1max = 0, j1sum = 0, j2max = 0, j2sum = 0, jn = 0;
+  for (int b = 0; b < ANALYTIC_BLOCKS; b++) {
+    const double* v = &st[(size_t)b * 8];
+    umax = std::max(umax, v[0]);
+    usum += v[1];
+    un += v[2];
+    j1max = std::max(j1max, v[3]);
+    j1sum += v[4];
+    j2max = std::max(j2max, v[5]);
+    j2sum += v[6];
+    jn += v[7];
+  }
+  stats[0] = umax;
+  stats[1] = usum / un;
+  stats[2] = j1max;
+  stats[3] = j1sum / jn;
+  stats[4] = j2max;
+  stats[5] = j2sum / jn;
   return EP2D_OK;
 }
 

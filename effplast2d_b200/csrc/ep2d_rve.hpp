@@ -88,6 +88,9 @@ class Rve {
   int get_field(int field, double* host) const;
   int set_field(int field, const double* host);
   int static_fields(double* unu, double* j1, double* j2);
+  // SaveAnStatic2D's analytic fields and error statistics (EffPlast2D.cu:1060-1292)
+  int analytic_fields(double delta_p, double tau_infty, double* uan, double* eu, double* j1an, double* j2an,
+                      double* ej1, double* ej2, double stats[6]);
 
   // state
   ep2d_params prm{};

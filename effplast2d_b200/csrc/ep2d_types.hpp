@@ -53,4 +53,16 @@ cudaError_t launch_gather(const Geo& g, const F64Fields& f, int src, const unsig
 cudaError_t launch_static_fields(const Geo& g, const F64Fields& f, int src, double* unu, double* j1, double* j2,
                                  cudaStream_t stream);
 
+// Scalars of the analytic static solution (SaveAnStatic2D, EffPlast2D.cu:1062-1078).
+struct AnParams {
+  double deltaP, tauInfty, Y, rad, G0, K0;
+  double xi, kappa, c0, rx, ry, Rx, Ry, Rmin, Rmax, eps;
+  int hydro;  // isHydroStatic (EffPlast2D.cu:1062-1064)
+};
+
+constexpr int ANALYTIC_BLOCKS = 592;  // 4 x 148 SMs; stats[ANALYTIC_BLOCKS][8]
+cudaError_t launch_analytic(const Geo& g, const AnParams& a, const double* unu, const double* j1nu, const double* j2nu,
+                            double* uan, double* eu, double* j1an, double* j2an, double* ej1, double* ej2,
+                            double* stats, cudaStream_t stream);
+
 }  // namespace ep2d

@@ -21,7 +21,7 @@ EXPORTS = (
     "ep2d_version", "ep2d_last_error", "ep2d_device_count", "ep2d_read_pa", "ep2d_make_pa",
     "ep2d_field_dims", "ep2d_create", "ep2d_destroy", "ep2d_iterate", "ep2d_get_field",
     "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
-    "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_abi_sizes", "ep2d_get_stats",
+    "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
 )
 
 
@@ -56,6 +56,7 @@ def lib():
         L.ep2d_get_check_errors.argtypes = [vp, i32, i32, P(d), i32, P(i32)]
         L.ep2d_compute_eff_moduli.argtypes = [vp, d, P(d), i32, P(_abi.Result)]
         L.ep2d_static_fields.argtypes = [vp, P(d), P(d), P(d)]
+        L.ep2d_analytic_fields.argtypes = [vp, d, d] + [P(d)] * 7
         L.ep2d_abi_sizes.argtypes = [P(i64), i32]
         L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64)]
         _lib = L
@@ -173,6 +174,17 @@ class Solver:
         j2 = np.zeros((ny - 1, nx - 1))
         _check(lib().ep2d_static_fields(self._h, _dptr(unu), _dptr(j1), _dptr(j2)))
         return {"UnuAbs": unu, "J1nu": j1, "J2nu": j2}
+
+    def analytic_fields(self, delta_p, tau_infty):
+        nx, ny = self.nx, self.ny
+        out = {k: np.zeros((ny, nx)) for k in ("UanAbs", "errorUabs")}
+        out.update({k: np.zeros((ny - 1, nx - 1)) for k in ("J1an", "J2an", "errorJ1", "errorJ2")})
+        st = np.zeros(6)
+        _check(lib().ep2d_analytic_fields(self._h, float(delta_p), float(tau_infty),
+                                          *[_dptr(out[k]) for k in ("UanAbs", "errorUabs", "J1an", "J2an",
+                                                                     "errorJ1", "errorJ2")], _dptr(st)))
+        out["stats"] = st
+        return out
 
     def stats(self):
         ms = ctypes.c_double()

@@ -187,6 +187,17 @@ int ep2d_compute_eff_moduli(ep2d_handle* h, double init_load_value, const double
  * displacements zeroed inside the pores (EffPlast2D.cu:514-547). */
 int ep2d_static_fields(ep2d_handle* h, double* unu_abs, double* j1nu, double* j2nu);
 
+/* SaveAnStatic2D's analytic part (EffPlast2D.cu:1060-1292): the Yarushina (2010)
+ * displacement magnitude at nodes (nx*ny) and stress invariants J1, J2 at corners
+ * ((nx-1)*(ny-1)) for the far-field pressure delta_p and shear tau_infty, the relative
+ * error maps against the current numerical fields (cut to -0.5 above 0.5, as the
+ * reference does), and stats = {Uabs max, avg, J1 max, avg, J2 max, avg}.  The
+ * reference computes these only for one pore (nPores == 1); the load type of the last
+ * ep2d_compute_eff_moduli call selects the hydrostatic branch. */
+int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, double* uan_abs,
+                         double* error_uabs, double* j1an, double* j2an, double* error_j1,
+                         double* error_j2, double stats[6]);
+
 /* sizeof(ep2d_params), sizeof(ep2d_step_record), sizeof(ep2d_moduli), sizeof(ep2d_result)
  * into out[0..n); returns the number of structs (4).  Lets a binding check its layout. */
 int ep2d_abi_sizes(int64_t* out, int32_t n);

@@ -103,6 +103,26 @@ def test_static_fields():
         assert np.max(np.abs(sg[k] - so[k])) <= 1e-9 * np.max(np.abs(so[k])), k
 
 
+@pytest.mark.parametrize("lt", [[1.0, 1.0, 0.0], [1.0, 0.7, 0.2]], ids=["hydrostatic", "shear"])
+def test_analytic_fields(lt):
+    # SaveAnStatic2D's analytic part (one pore): device complex FP64 vs the oracle's C99
+    # complex restatement.  Different complex-function implementations: agree to 1e-10.
+    nx = 64
+    pa = oracle.make_pa(20.0, 20.0, nx, nx, g0=0.5, yield_stress=1e-5, porosity=0.01, n_pores=1)
+    g = ep.Solver(nx, nx, pa, nl=2, niter=3000, eiter=1e-9, check_every=1000)
+    o = oracle.Oracle(nx, nx, pa, nl=2, niter=3000, eiter=1e-9, check_every=1000)
+    g.compute_eff_moduli(-6e-5, lt, 1)
+    o.compute_eff_moduli(-6e-5, lt, 1)
+    r0 = o.record(0, 0)
+    ga = g.analytic_fields(r0["delta_p"], r0["tau_infty"])
+    oa = o.static_fields(r0["delta_p"], r0["tau_infty"])
+    for k in ("UanAbs", "J1an", "J2an"):
+        assert np.max(np.abs(ga[k] - oa[k])) <= 1e-10 * np.max(np.abs(oa[k])), k
+    for k in ("errorUabs", "errorJ1", "errorJ2"):
+        assert np.max(np.abs(ga[k] - oa[k])) <= 1e-7, k
+    assert np.allclose(ga["stats"], oa["stats"], rtol=1e-7, atol=0)
+
+
 def test_increment_before_preload_is_rejected():
     nx = 32
     pa = oracle.make_pa(20.0, 20.0, nx, nx)
