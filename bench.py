@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""bench.py -- converged RVE solves/s of the EffPlast2D pseudo-transient solver on B200.
+
+One step = one complete homogenisation of the headline workload (the reference's
+ComputeEffModuli chain: preload over n_time_steps, then the load increments, each
+iterated to EITER with the reference's checkpoint cadence), from rest.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own RVEs (independent
+units, no collective on the data path), timed between barriers; the time is the max
+over ranks; value = RVEs solved by all ranks / that time ("scaling": "weak").
+
+--impl reference times the reference algorithm on the host cores (the CPU restatement
+of EffPlast2D.cu, all threads) on a bounded sample of the same workload and converts its
+cell-update rate into solves/s with the iteration count of a full solve recorded from
+the reference's own run (tests/golden).  Rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# ---- workloads (synthetic by construction: the reference has no dataset) -----------
+WORKLOADS = {
+    # the configuration the metric is quoted on (1024^2, 3x3 pores, elastoplastic)
+    "cfg2": dict(n=1024, n_pores=3, porosity=0.01, g0=0.5, yield_stress=1e-5, load=-6e-5, load_type=(1.0, 1.0, 0.0),
+                 n_time_steps=2, nl=2, niter=5_000_000, eiter=1e-9, check_every=10_000,
+                 label="1024x1024 grid, 3x3 pores, porosity 0.01, K0=1 G0=0.5 Y=1e-5, preload -6e-5*[1,1,0] "
+                       "over 2 time steps + bulk increment (NL=2), eIter 1e-9"),
+    # config 3 geometry (2048^2, 4x4 pores, shear load, NL=3), larger than L2 in FP64
+    "cfg3": dict(n=2048, n_pores=4, porosity=0.02, g0=0.5, yield_stress=1e-5, load=-6e-5, load_type=(1.0, 1.0, 0.5),
+                 n_time_steps=1, nl=3, niter=5_000_000, eiter=1e-9, check_every=10_000,
+                 label="2048x2048 grid, 4x4 pores, porosity 0.02, K0=1 G0=0.5 Y=1e-5, preload -6e-5*[1,1,0.5] "
+                       "+ bulk and shear increments (NL=3), eIter 1e-9"),
+    # the reference's CPU-runnable case (elastic, one pore)
+    "cfg1": dict(n=128, n_pores=1, porosity=0.005, g0=0.5, yield_stress=1.0, load=-4e-5, load_type=(1.0, 1.0, 0.0),
+                 n_time_steps=1, nl=1, niter=100_000, eiter=1e-9, check_every=10_000,
+                 label="128x128 grid, 1 pore, porosity 0.005, K0=1 G0=0.5 Y=1, preload -4e-5*[1,1,0] (NL=1), "
+                       "eIter 1e-9"),
+}
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def make_pa(w):
+    from effplast2d_b200 import make_pa as lib_make_pa
+
+    n = w["n"]
+    return lib_make_pa(20.0, 20.0, n, n, g0=w["g0"], yield_stress=w["yield_stress"], porosity=w["porosity"],
+                       n_pores=w["n_pores"])
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload):
+    """DRAM bytes per launch of the iteration kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "iter_f64_%s.json" % workload)
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = str(device_index)
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9 and p[0] == self.dev:
+                self.rows.append(p)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_sample(w, seconds=12.0, threads=None):
+    """The CPU restatement of the reference on `threads` host threads, iterating the
+    workload's preloaded state: returns (cell updates per second, threads, description)."""
+    import numpy as np
+
+    import oracle
+
+    threads = threads or os.cpu_count() or 1
+    oracle.set_threads(threads)
+    n = w["n"]
+    pa = make_pa_oracle(w)
+    o = oracle.Oracle(n, n, pa, nl=w["nl"], niter=1, eiter=w["eiter"], check_every=w["check_every"])
+    dx = pa[0]
+    e = w["load"] / w["n_time_steps"]
+    xi = -0.5 * dx * n + dx * np.arange(n + 1)
+    yj = -0.5 * dx * n + dx * np.arange(n + 1)
+    o.set("Ux", np.broadcast_to(e * w["load_type"][0] * xi[None, :], (n, n + 1)))
+    o.set("Uy", np.broadcast_to(e * w["load_type"][1] * yj[:, None], (n + 1, n)))
+    o.iterate(2)
+    t = time.perf_counter()
+    o.iterate(10)
+    dt = time.perf_counter() - t
+    iters = max(10, int(seconds / max(dt / 10, 1e-9)))
+    t = time.perf_counter()
+    o.iterate(iters)
+    dt = time.perf_counter() - t
+    o.close()
+    rate = iters * n * n / dt
+    return rate, threads, "%d pseudo-time iterations of the %dx%d preloaded state (%.1f s)" % (iters, n, n, dt)
+
+
+def make_pa_oracle(w):
+    import oracle
+
+    n = w["n"]
+    return oracle.make_pa(20.0, 20.0, n, n, g0=w["g0"], yield_stress=w["yield_stress"], porosity=w["porosity"],
+                          n_pores=w["n_pores"])
+
+
+def run_reference(args, w):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    p = os.path.join(ROOT, "tests", "golden", args.workload + ".json")
+    if not os.path.exists(p):
+        print(json.dumps({"impl": "reference", "unavailable": "no recorded reference run of workload %s" % args.workload}))
+        return 0
+    meta = json.load(open(p))
+    total_iters = meta.get("total_iterations")
+    n = w["n"]
+    secs = float(os.environ.get("EP2D_REF_SAMPLE_S", "8"))
+    vals = []
+    desc = ""
+    threads = os.cpu_count() or 1
+    for k in range(args.warmup + args.steps):
+        rate, threads, desc = cpu_sample(w, seconds=secs if k >= args.warmup else 1.0)
+        if k >= args.warmup:
+            vals.append(rate)
+    rate = statistics.median(vals)
+    v = rate / (n * n * total_iters)
+    line = {
+        "impl": "reference", "metric": "converged RVE solves/s", "value": v, "unit": "RVE solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": w["label"], "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
+                         "sample": desc + "; solves/s = cell-update rate / (%d^2 cells x %d iterations per solve, "
+                                          "from the reference's own run)" % (n, total_iters)},
+        "e2e": {"value": v, "unit": "RVE solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, w):
+    import torch
+
+    import effplast2d_b200 as ep
+
+    world, rank, local = dist_setup()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    n = w["n"]
+    pa = make_pa(w)
+    lt = list(w["load_type"])
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # value: resident handle, each step = reset (a fresh object) + full chain
+    s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"], device=dev)
+    res = None
+    for _ in range(args.warmup):
+        s.reset()
+        res = s.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
+    st0 = s.stats()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        flush.zero_()
+        s.reset()
+        res = s.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
+    torch.cuda.synchronize()
+    ev1.record()
+    ev1.synchronize()
+    barrier()
+    clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    st1 = s.stats()
+    iters_per_solve = res["total_iterations"]
+
+    # e2e: through the C ABI with host buffers: create (H2D of the pore-edge index list,
+    # device mask setup), solve, copy the output fields the reference writes (Pc, tauXXc)
+    # to host memory, destroy
+    h2d = 8 * 20 * int(w["n_pores"]) ** 2
+    d2h = 2 * n * n * 8
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        flush.zero_()
+        s2 = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
+                       device=dev)
+        s2.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
+        s2.get("P")
+        s2.get("tauXX")
+        s2.close()
+    torch.cuda.synchronize()
+    e1.record()
+    e1.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+
+    # max over ranks
+    t = torch.tensor([ms, e2e_ms, float(st1["all_launches"] - st0["all_launches"])], dtype=torch.float64,
+                     device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, e2e_ms = float(mx[0]), float(mx[1])
+        launches = int(sm[2])
+    else:
+        launches = int(t[2])
+
+    # roofline of the fused iteration kernel over the timed region
+    it_launches = st1["launches"] - st0["launches"]
+    it_ms = st1["kernel_ms"] - st0["kernel_ms"]
+    avg_launch_s = it_ms / 1000.0 / max(it_launches, 1)
+    bytes_alg = 64 * n * n  # Ux, Uy, Vx, Vy read once and written once, FP64
+    achieved = bytes_alg / avg_launch_s / 1e9
+    peak, peak_kind = measured_peaks()
+
+    line = None
+    if rank == 0:
+        total = world * args.steps
+        value = total / (ms / 1000.0)
+        line = {
+            "metric": "converged RVE solves/s", "value": value, "unit": "RVE solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "description": w["label"],
+                       "iterations_per_solve": iters_per_solve, "global_batch": world,
+                       "l2": "256 MB buffer written between steps", "parallelism": "rve-sharded x%d" % world},
+            "e2e": {"value": total / (e2e_ms / 1000.0), "unit": "RVE solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
+                         "kernel": "k_iter_f64 (fused stress + J2 return + momentum update)",
+                         "algorithmic_bytes_per_launch": bytes_alg, "avg_launch_us": avg_launch_s * 1e6,
+                         "peak_source": peak_kind},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "cell_updates_per_s": iters_per_solve * n * n * total / (ms / 1000.0),
+            "moduli": {"kd": res["num"]["kd"], "kphi": res["num"]["kphi"]},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            rate, threads, desc = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_S", "12")))
+            v = rate / (n * n * iters_per_solve)
+            line["cpu_baseline"] = {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
+                                    "sample": desc + "; converted with %d iterations per solve" % iters_per_solve}
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+def run_kernel_only(args, w):
+    """Exactly N pseudo-time iterations of the workload's preload step (no convergence
+    test): the fixed, short launch sequence used for ncu captures and for timing the
+    fused iteration kernel alone."""
+    import torch
+
+    import effplast2d_b200 as ep
+
+    n = w["n"]
+    iters = args.kernel_only
+    s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=iters, eiter=0.0, check_every=iters, device=0)
+    s.solve_step(0, w["load"], list(w["load_type"]), 1)  # warm-up and preload
+    st0 = s.stats()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    s.solve_step(0, w["load"], list(w["load_type"]), 1)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    st1 = s.stats()
+    per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(st1["launches"] - st0["launches"], 1)
+    bytes_alg = 64 * n * n
+    peak, kind = measured_peaks()
+    print(json.dumps({"workload": args.workload, "iterations": iters, "avg_launch_us": per * 1e3,
+                      "achieved_gbs": bytes_alg / (per / 1e3) / 1e9, "peak_gbs": peak, "peak_source": kind,
+                      "frac": bytes_alg / (per / 1e3) / 1e9 / peak, "wall_s": wall,
+                      "cell_updates_per_s": n * n / (per / 1e3)}))
+    s.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
+                    help="run N iterations of the workload's preload step and report the kernel timing")
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.kernel_only:
+        return run_kernel_only(args, w)
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_ours(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

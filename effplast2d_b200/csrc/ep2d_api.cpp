@@ -106,6 +106,11 @@ int ep2d_destroy(ep2d_handle* h) {
   })
 }
 
+int ep2d_reset(ep2d_handle* h) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  EP2D_GUARD({ return h->rve.reset(); })
+}
+
 int ep2d_iterate(ep2d_handle* h, int64_t n_iter) {
   if (!h || n_iter < 0) return fail(EP2D_ERR_ARG, "bad handle or count");
   EP2D_GUARD({
@@ -178,10 +183,12 @@ int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, doubl
   })
 }
 
-int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t* cell_updates) {
+int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t* cell_updates,
+                   int64_t* all_launches) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
   if (kernel_ms) *kernel_ms = h->rve.kernel_ms;
   if (launches) *launches = h->rve.launches;
+  if (all_launches) *all_launches = h->rve.launches + h->rve.aux_launches;
   if (cell_updates) *cell_updates = h->rve.cell_updates;
   return EP2D_OK;
 }

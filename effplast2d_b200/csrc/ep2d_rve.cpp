@@ -407,10 +407,31 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
     EP2D_CK(cudaMemcpyAsync(d_idx, codes.data(), codes.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice,
                             stream));
   EP2D_CK(launch_mask(g, mask, stream));
+  aux_launches += 1;
   EP2D_CK(cudaEventCreate(&ev_[0]));
   EP2D_CK(cudaEventCreate(&ev_[1]));
   EP2D_CK(cudaStreamSynchronize(stream));
   cur = 0;
+  return EP2D_OK;
+}
+
+int Rve::reset() {
+  if (!dmem) return fail(EP2D_ERR_STATE, "handle is not initialised");
+  DeviceScope ds(device);
+  // the 13 field arrays are contiguous at the start of the allocation
+  const size_t bytes = reinterpret_cast<char*>(const_cast<uint8_t*>(f.mask)) - static_cast<char*>(dmem);
+  EP2D_CK(cudaMemsetAsync(dmem, 0, bytes, stream));
+  EP2D_CK(cudaStreamSynchronize(stream));
+  cur = 0;
+  for (int s = 0; s < EP2D_MAX_NL; s++) {
+    nts[s] = 0;
+    rec[s].clear();
+    checks[s].clear();
+  }
+  ces[0] = ces[1] = ces[2] = 0.0;
+  load_type_[0] = load_type_[1] = load_type_[2] = 0.0;
+  have_step0 = false;
+  an = an_per = num = num_per = ep2d_moduli{0.0, 0.0, 0.0};
   return EP2D_OK;
 }
 
@@ -517,6 +538,7 @@ int Rve::begin_time_step(int step, int it, double lsv, const double lt[3], int n
   std::memcpy(r.macro_strain, ces, sizeof(ces));
   const int zero_first = (step == 0 && it == 0) ? 1 : 0;
   EP2D_CK(launch_preload(g, f, cur, dUxdx, dUydy, dUxdy, zero_first, stream));
+  aux_launches += 1;
   return EP2D_OK;
 }
 
@@ -528,6 +550,7 @@ int Rve::finish_time_step(int step, int it) {
   EP2D_CK(launch_average(g, f, cur, d.nu0, perOffsetX, perOffsetY, d_partials, d_out, stream));
   EP2D_CK(launch_boundary(g, f, d_out + NAVG, stream));
   EP2D_CK(launch_gather(g, f, cur, d_idx, (int)holes.size(), d_out + 2 * NAVG, stream));
+  aux_launches += holes.empty() ? 3 : 4;
   EP2D_CK(cudaMemcpyAsync(h_pin, d_out, (2 * NAVG + holes.size()) * sizeof(double), cudaMemcpyDeviceToHost, stream));
   EP2D_CK(cudaStreamSynchronize(stream));
   finish_record(d, prm.nx, prm.ny, prm.nl, step, h_pin, h_pin + NAVG, holes, h_pin + 2 * NAVG, &r, &an, &an_per);

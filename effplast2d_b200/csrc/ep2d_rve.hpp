@@ -66,6 +66,7 @@ class Rve {
   // allocate and initialise (constructor of the reference); stream may be null: own one
   int create(const ep2d_params& p, cudaStream_t stream = nullptr);
   void release();
+  int reset();  // zero all fields and records (a freshly constructed object)
 
   // bytes of device memory one RVE with these parameters holds
   static size_t footprint(const ep2d_params& p);
@@ -113,7 +114,8 @@ class Rve {
 
   // statistics
   double kernel_ms = 0.0;
-  int64_t launches = 0;
+  int64_t launches = 0;      // fused iteration kernel
+  int64_t aux_launches = 0;  // preload, averaging, boundary, gather, mask
   int64_t cell_updates = 0;
 
   // device scratch

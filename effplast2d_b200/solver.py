@@ -19,7 +19,7 @@ _lib = None
 # every symbol include/ep2d.h declares
 EXPORTS = (
     "ep2d_version", "ep2d_last_error", "ep2d_device_count", "ep2d_read_pa", "ep2d_make_pa",
-    "ep2d_field_dims", "ep2d_create", "ep2d_destroy", "ep2d_iterate", "ep2d_get_field",
+    "ep2d_field_dims", "ep2d_create", "ep2d_destroy", "ep2d_reset", "ep2d_iterate", "ep2d_get_field",
     "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
 )
@@ -48,6 +48,7 @@ def lib():
         L.ep2d_field_dims.argtypes = [i32, i32, i32, P(i32), P(i32)]
         L.ep2d_create.argtypes = [P(_abi.Params), P(vp)]
         L.ep2d_destroy.argtypes = [vp]
+        L.ep2d_reset.argtypes = [vp]
         L.ep2d_iterate.argtypes = [vp, i64]
         L.ep2d_get_field.argtypes = [vp, i32, P(d)]
         L.ep2d_set_field.argtypes = [vp, i32, P(d)]
@@ -58,7 +59,7 @@ def lib():
         L.ep2d_static_fields.argtypes = [vp, P(d), P(d), P(d)]
         L.ep2d_analytic_fields.argtypes = [vp, d, d] + [P(d)] * 7
         L.ep2d_abi_sizes.argtypes = [P(i64), i32]
-        L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64)]
+        L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64), P(i64)]
         _lib = L
     return _lib
 
@@ -137,6 +138,9 @@ class Solver:
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(h, w)
         _check(lib().ep2d_set_field(self._h, _abi.FIELD_ID[field], _dptr(a)))
 
+    def reset(self):
+        _check(lib().ep2d_reset(self._h))
+
     def iterate(self, n):
         _check(lib().ep2d_iterate(self._h, int(n)))
 
@@ -188,7 +192,8 @@ class Solver:
 
     def stats(self):
         ms = ctypes.c_double()
-        la = ctypes.c_int64()
-        cu = ctypes.c_int64()
-        _check(lib().ep2d_get_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(cu)))
-        return {"kernel_ms": ms.value, "launches": la.value, "cell_updates": cu.value}
+        la, cu, al = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().ep2d_get_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(cu),
+                                    ctypes.byref(al)))
+        return {"kernel_ms": ms.value, "launches": la.value, "cell_updates": cu.value,
+                "all_launches": al.value}

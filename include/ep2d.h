@@ -151,6 +151,10 @@ int ep2d_field_dims(int32_t nx, int32_t ny, int32_t field, int32_t* width, int32
 int ep2d_create(const ep2d_params* params, ep2d_handle** out);
 /* EffPlast2D::~EffPlast2D (EffPlast2D.cu:1613-1658) */
 int ep2d_destroy(ep2d_handle* h);
+/* Return a handle to the state of a freshly constructed object (EffPlast2D.cu:1585-1604:
+ * every field zero, no records) without reallocating.  The reference object keeps its
+ * velocities across ComputeEffModuli calls; a new object starts from rest, as this does. */
+int ep2d_reset(ep2d_handle* h);
 
 /* Exactly n pseudo-time iterations of the reference's kernel sequence
  * ComputeStress -> [ComputeJ2 -> ComputePlasticity if nl > 1] -> ComputeDisp
@@ -202,9 +206,12 @@ int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, doubl
  * into out[0..n); returns the number of structs (4).  Lets a binding check its layout. */
 int ep2d_abi_sizes(int64_t* out, int32_t n);
 
-/* device time spent in the iteration kernels of this handle so far (ms), and the
- * number of kernel launches issued for them */
-int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t* cell_updates);
+/* Counters of this handle since creation: device time of the iteration loops measured
+ * with CUDA events on the handle's stream (ms), launches of the fused iteration kernel,
+ * cell updates (nx*ny per iteration), and all kernel launches (iteration kernel plus
+ * preload, reductions and gathers).  Any pointer may be NULL. */
+int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* iter_launches, int64_t* cell_updates,
+                   int64_t* all_launches);
 
 #ifdef __cplusplus
 }

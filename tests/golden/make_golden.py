@@ -143,7 +143,7 @@ def parse_records(path):
     return head, recs, mod
 
 
-def chain_case(out, case, fields_keep=None):
+def chain_case(out, case, fields_keep=None, with_cli=True):
     name, cfg, n, npores, phi, g0, Y, load, lt, nts = case
     pa = oracle.make_pa(20.0, 20.0, n, n, g0=g0, yield_stress=Y, porosity=phi, n_pores=npores)
     args = ["%.17g" % load, "%.17g" % lt[0], "%.17g" % lt[1], "%.17g" % lt[2], str(nts), "%.17g" % (0.1 * load)]
@@ -164,14 +164,32 @@ def chain_case(out, case, fields_keep=None):
     keep = fields_keep or list(FIELDS)
     for f in keep:
         res["f_" + f] = read_field(dump, f, n, n)
-    shutil.rmtree(work)
-    # 2) the reference CLI itself: stdout (17 digits), EffPlast2D.log, data/*.dat
-    work = tempfile.mkdtemp()
-    os.makedirs(os.path.join(work, "data"))
-    np.asarray(pa, dtype="<f8").tofile(os.path.join(work, "data", "pa.dat"))
-    stdout_c, dt2 = run([os.path.join(REF, "cli_" + cfg)] + args, cwd=work, timeout=7200)
+    if with_cli:
+        shutil.rmtree(work)
+        # 2) the reference CLI itself: stdout (17 digits), EffPlast2D.log, data/*.dat
+        work = tempfile.mkdtemp()
+        os.makedirs(os.path.join(work, "data"))
+        np.asarray(pa, dtype="<f8").tofile(os.path.join(work, "data", "pa.dat"))
+        stdout_c, dt2 = run([os.path.join(REF, "cli_" + cfg)] + args, cwd=work, timeout=7200)
+    else:
+        # the harness ran the same ComputeEffModuli in `work`: its stdout (6 digits),
+        # EffPlast2D.log and data/*.dat are the reference's outputs of this case
+        stdout_c, dt2 = stdout_h, 0.0
     meta["cli_seconds"] = dt2
     meta["cli_stdout"] = stdout_c
+    # iterations of the whole solve: the converged checkpoint, or NITER when a time step
+    # ends on the iteration cap (EffPlast2D.cu:389-428)
+    total, last = 0, 0
+    for line in stdout_c.splitlines():
+        if line.strip().startswith("Iteration "):
+            last = int(line.split()[1].rstrip(":"))
+        elif line.startswith("Number of iterations is"):
+            total += int(line.split()[-1])
+            last = 0
+        elif line.startswith("WARNING: Maximum number of iterations"):
+            total += MACROS[cfg]["NITER"]
+            last = 0
+    meta["total_iterations"] = total
     meta["cli_log"] = open(os.path.join(work, "EffPlast2D.log")).read()
     dats = sorted(os.listdir(os.path.join(work, "data")))
     meta["cli_dat_files"] = dats
@@ -214,7 +232,7 @@ def main():
         if only is None or c[0] in only:
             chain_case(out, c)
     if with_cfg2 or (only and "cfg2" in only):
-        chain_case(out, CFG2, fields_keep=["P", "tauXX", "tauXY", "Ux", "Uy"])
+        chain_case(out, CFG2, fields_keep=["P", "tauXX", "tauXY", "Ux", "Uy"], with_cli=False)
 
 
 if __name__ == "__main__":

@@ -23,22 +23,32 @@ SCALARS = ["delta_p", "delta_p_per", "tau_infty", "hole_area_pi", "internal_hole
 VECTORS = ["macro_strain", "sigma", "sigma_per", "eps_per"]
 
 
-def close(a, b, tol):
+STRESS_LIKE = {"delta_p", "delta_p_per", "tau_infty", "sigma", "sigma_per"}
+
+
+def close(a, b, tol, atol=0.0):
     if a == b:
         return True
     if isinstance(a, float) and (math.isnan(a) or math.isnan(b)):
         return math.isnan(a) and math.isnan(b)
-    return abs(a - b) <= tol * max(abs(b), 1e-300) or abs(a - b) < 1e-300
+    return abs(a - b) <= tol * abs(b) + atol
 
 
 def compare_records(rg, ro, tol):
+    """Values that are rounding noise (tau_infty under a hydrostatic load, ~1e-21; the
+    error of a converged state, ~1e-16) get absolute floors: 1e-9 of the record's stress
+    scale for stress-like values, 1e-13 for the convergence error."""
     for k in ("iterations", "converged", "n_checks", "step", "time_step"):
         assert rg[k] == ro[k], k
+    scale = max([abs(v) for v in ro["sigma"]] + [abs(ro["delta_p"])]) or 1.0
+    strain = max(abs(v) for v in ro["macro_strain"]) or 1.0
     for k in SCALARS:
-        assert close(rg[k], ro[k], tol), (k, rg[k], ro[k])
+        atol = 1e-9 * scale if k in STRESS_LIKE else (1e-13 if k == "error" else 0.0)
+        assert close(rg[k], ro[k], tol, atol), (k, rg[k], ro[k])
     for k in VECTORS:
+        atol = 1e-9 * scale if k in STRESS_LIKE else 1e-9 * strain
         for a, b in zip(rg[k], ro[k]):
-            assert close(a, b, tol) or abs(a - b) < 1e-14 * max(map(abs, ro[k]) or [1.0]), (k, rg[k], ro[k])
+            assert close(a, b, tol, atol), (k, rg[k], ro[k])
 
 
 CASES = [
@@ -63,7 +73,7 @@ def test_eff_moduli_chain(case):
             compare_records(g.record(s, t), o.record(s, t), 1e-9)
             eg, eo = g.check_errors(s, t), o.check_errors(s, t)
             assert len(eg) == len(eo)
-            assert np.allclose(eg, eo, rtol=1e-8, atol=0)
+            assert np.allclose(eg, eo, rtol=1e-8, atol=1e-13)
     for kind in ("num", "num_per", "an", "an_per"):
         keys = ["kphi", "kd"] + (["g"] if nl == 3 else [])
         for k in keys:

@@ -119,6 +119,6 @@ def test_homogeneous_affine_is_equilibrium():
     g.set("Ux", st["Ux"])
     g.set("Uy", st["Uy"])
     g.iterate(50)
-    assert np.max(np.abs(g.get("Vx"))) < 1e-18
+    assert np.max(np.abs(g.get("Vx"))) < 1e-16  # rounding of the affine differences only
     P = g.get("P")
     assert np.allclose(P, P[1, 1], rtol=1e-12, atol=0)
