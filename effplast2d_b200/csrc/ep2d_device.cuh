@@ -122,225 +122,6 @@ __global__ void k_preload(Geo g, double* ux0, double* ux1, double* uy0, double* 
 }
 
 // ---------------------------------------------------------------------------------
-// The fused iteration kernel (north-star items a and b).
-//
-// One launch = one pseudo-time iteration of the reference's four kernels
-// ComputeStress (:37-98) -> ComputeJ2 (:100-145) -> ComputePlasticity (:147-177) ->
-// ComputeDisp (:3-35).  Each CTA owns a TX x TY block of nodes and of the faces with
-// the same (i, j); it stages the displacement halo (radius 2) and the masks in shared
-// memory, computes trial stresses on the halo region, applies the J2 radial return
-// (nodes with the averaged tauXY, corners with averaged tauXX/tauYY), and updates the
-// velocities and displacements of its own faces.  Stresses never touch HBM except on
-// RECORD launches (checkpoints and the last iteration), which also write the stress
-// fields and fold max|V| into vmax for the convergence norm (north-star item c).
-//
-// Arithmetic is written expression by expression as in the reference kernels.
-// ---------------------------------------------------------------------------------
-template <int TX, int TY>
-struct TileSmem {
-  static constexpr int UW = TX + 3, UH = TY + 3;  // Ux, Uy, mask halo tiles
-  static constexpr int SW = TX + 2, SH = TY + 2;  // node stress and corner stress tiles
-  static constexpr int FW = TX + 1, FH = TY + 1;  // return factors
-  double ux[UH][UW];
-  double uy[UH][UW];
-  double p[SH][SW];
-  double xx[SH][SW];
-  double yy[SH][SW];
-  double xy[SH][SW];
-  double fn[FH][FW];
-  double fc[FH][FW];
-  uint8_t m[UH][UW];
-};
-
-__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
-  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
-}
-
-template <int TX, int TY, bool PLASTIC, bool RECORD>
-__global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
-  using S = TileSmem<TX, TY>;
-  constexpr int UW = S::UW, UH = S::UH, SW = S::SW, SH = S::SH, FW = S::FW, FH = S::FH;
-  constexpr int NT = 256;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S& s = *reinterpret_cast<S*>(smem_raw);
-
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int nx = g.nx, ny = g.ny;
-  const size_t pitch = (size_t)g.pitch;
-  const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
-  const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
-  double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
-  double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
-
-  // ---- A: stage Ux (i in [i0-1, i0+TX+1], j in [j0-2, j0+TY]),
-  //         Uy (i in [i0-2, i0+TX], j in [j0-1, j0+TY+1]) and the mask
-  //         (nodes i in [i0-2, i0+TX], j in [j0-2, j0+TY]); zero outside the domain.
-  for (int e = tid; e < UH * UW; e += NT) {
-    const int lj = e / UW, li = e - lj * UW;
-    int i = i0 - 1 + li, j = j0 - 2 + lj;
-    s.ux[lj][li] = (i >= 0 && i <= nx && j >= 0 && j < ny) ? ux[j * pitch + i] : 0.0;
-    i = i0 - 2 + li;
-    j = j0 - 1 + lj;
-    s.uy[lj][li] = (i >= 0 && i < nx && j >= 0 && j <= ny) ? uy[j * pitch + i] : 0.0;
-    j = j0 - 2 + lj;
-    s.m[lj][li] = (i >= 0 && i < nx && j >= 0 && j < ny) ? f.mask[j * pitch + i] : (uint8_t)0;
-  }
-  __syncthreads();
-
-  const double dX = g.dX, dY = g.dY;
-  // ---- B: trial stresses.  Nodes (i0-1+li, j0-1+lj) and corners (i0-2+li, j0-2+lj).
-  for (int e = tid; e < SH * SW; e += NT) {
-    const int lj = e / SW, li = e - lj * SW;
-    {
-      const int i = i0 - 1 + li, j = j0 - 1 + lj;
-      double pv = 0.0, xv = 0.0, yv = 0.0;
-      if (i >= 0 && i < nx && j >= 0 && j < ny) {
-        const double uxa = s.ux[lj + 1][li], uxb = s.ux[lj + 1][li + 1];
-        const double uya = s.uy[lj][li + 1], uyb = s.uy[lj + 1][li + 1];
-        const uint8_t m = s.m[lj + 1][li + 1];
-        const double K = (m & M_MAT) ? g.Kp : g.K0;
-        const double G = (m & M_MAT) ? g.Gp : g.G0;
-        const double divU = (uxb - uxa) / dX + (uyb - uya) / dY;
-        pv = 0.0 - K * divU;  // P0 - K divU with P0 == 0
-        xv = 2.0 * G * ((uxb - uxa) / dX - divU / 3.0);
-        yv = 2.0 * G * ((uyb - uya) / dY - divU / 3.0);
-        if (m & M_NODE) {
-          pv = 0.0;
-          xv = 0.0;
-          yv = 0.0;
-        }
-      }
-      s.p[lj][li] = pv;
-      s.xx[lj][li] = xv;
-      s.yy[lj][li] = yv;
-    }
-    {
-      const int ci = i0 - 2 + li, cj = j0 - 2 + lj;
-      double t = 0.0;
-      if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
-        const uint8_t m00 = s.m[lj][li], m10 = s.m[lj][li + 1], m01 = s.m[lj + 1][li], m11 = s.m[lj + 1][li + 1];
-        const double Gs = ((m00 & M_MAT) ? g.Gp : g.G0) + ((m10 & M_MAT) ? g.Gp : g.G0) +
-                          ((m01 & M_MAT) ? g.Gp : g.G0) + ((m11 & M_MAT) ? g.Gp : g.G0);
-        t = 0.25 * Gs * ((s.ux[lj + 1][li] - s.ux[lj][li]) / dY + (s.uy[lj][li + 1] - s.uy[lj][li]) / dX);
-        if (m00 & M_CORNER) t = 0.0;
-      }
-      s.xy[lj][li] = t;
-    }
-  }
-  __syncthreads();
-
-  // ---- C: J2 radial return (only when NL > 1, EffPlast2D.cu:392-397).
-  if (PLASTIC) {
-    const double coh = g.coh;
-    for (int e = tid; e < FH * FW; e += NT) {
-      const int lj = e / FW, li = e - lj * FW;
-      {  // node (i0-1+li, j0-1+lj): tauXYav from the 2x2 corner block (:109-135)
-        const int i = i0 - 1 + li, j = j0 - 1 + lj;
-        double fn = 1.0;
-        if (i >= 0 && i < nx && j >= 0 && j < ny) {
-          const int ci = min(max(i - 1, 0), nx - 3), cj = min(max(j - 1, 0), ny - 3);
-          const int a = ci - (i0 - 2), b = cj - (j0 - 2);
-          double tav = 0.25 * (s.xy[b][a] + s.xy[b][a + 1] + s.xy[b + 1][a] + s.xy[b + 1][a + 1]);
-          double xv = s.xx[lj][li], yv = s.yy[lj][li];
-          double J2 = sqrt(xv * xv + yv * yv + 2.0 * tav * tav);
-          if (J2 > coh) {
-            fn = coh / J2;
-            if (RECORD) {
-              xv *= fn;
-              yv *= fn;
-              tav *= fn;
-              J2 = sqrt(xv * xv + yv * yv + 2.0 * tav * tav);
-            }
-          }
-          if (RECORD && li >= 1 && lj >= 1) {
-            f.txyav[j * pitch + i] = tav;
-            f.j2[j * pitch + i] = J2;
-          }
-        }
-        s.fn[lj][li] = fn;
-      }
-      {  // corner (i0-1+li, j0-1+lj): J2XY from averaged tauXX, tauYY (:138-144)
-        const int ci = i0 - 1 + li, cj = j0 - 1 + lj;
-        double fc = 1.0;
-        if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
-          const double sx = s.xx[lj][li] + s.xx[lj][li + 1] + s.xx[lj + 1][li] + s.xx[lj + 1][li + 1];
-          const double sy = s.yy[lj][li] + s.yy[lj][li + 1] + s.yy[lj + 1][li] + s.yy[lj + 1][li + 1];
-          const double t = s.xy[lj + 1][li + 1];
-          const double J2XY = sqrt(0.0625 * sx * sx + 0.0625 * sy * sy + 2.0 * t * t);
-          if (J2XY > coh) fc = coh / J2XY;
-          if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = J2XY;
-        }
-        s.fc[lj][li] = fc;
-      }
-    }
-    __syncthreads();
-    for (int e = tid; e < FH * FW; e += NT) {
-      const int lj = e / FW, li = e - lj * FW;
-      const double fn = s.fn[lj][li];
-      s.xx[lj][li] *= fn;
-      s.yy[lj][li] *= fn;
-      s.xy[lj + 1][li + 1] *= s.fc[lj][li];
-    }
-    __syncthreads();
-  }
-
-  // ---- D: damped momentum update and U += V dt on the CTA's own faces.
-  const double dT = g.dT;
-  const double cX = 1.0 - dT * g.dampX, cY = 1.0 - dT * g.dampY;
-  const double dtr = dT / g.rho;
-  double vmx = 0.0, vmy = 0.0;
-  for (int e = tid; e < TX * TY; e += NT) {
-    const int lj = e / TX, li = e - lj * TX;
-    const int i = i0 + li, j = j0 + lj;
-    if (i >= nx || j >= ny) continue;
-    const size_t q = j * pitch + i;
-    double vx = f.vx[q];
-    if (i > 0 && j > 0 && j < ny - 1) {
-      vx = vx * cX + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj + 1][li] + s.xx[lj + 1][li + 1] - s.xx[lj + 1][li]) / dX +
-                            (s.xy[lj + 2][li + 1] - s.xy[lj + 1][li + 1]) / dY);
-      f.vx[q] = vx;
-    }
-    uxo[q] = s.ux[lj + 2][li + 1] + vx * dT;
-    double vy = f.vy[q];
-    if (i > 0 && i < nx - 1 && j > 0) {
-      vy = vy * cY + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj][li + 1] + s.yy[lj + 1][li + 1] - s.yy[lj][li + 1]) / dY +
-                            (s.xy[lj + 1][li + 2] - s.xy[lj + 1][li + 1]) / dX);
-      f.vy[q] = vy;
-    }
-    uyo[q] = s.uy[lj + 1][li + 2] + vy * dT;
-    if (i == nx - 1) {  // face column i = nx of Ux/Vx: never updated by the reference
-      const size_t q2 = j * pitch + nx;
-      uxo[q2] = s.ux[lj + 2][li + 2];
-      if (RECORD) vmx = fmax(vmx, fabs(f.vx[q2]));
-    }
-    if (j == ny - 1) {  // face row j = ny of Uy/Vy
-      const size_t q3 = (size_t)ny * pitch + i;
-      uyo[q3] = s.uy[lj + 2][li + 2];
-      if (RECORD) vmy = fmax(vmy, fabs(f.vy[q3]));
-    }
-    if (RECORD) {
-      vmx = fmax(vmx, fabs(vx));
-      vmy = fmax(vmy, fabs(vy));
-      f.p[q] = s.p[lj + 1][li + 1];
-      f.txx[q] = s.xx[lj + 1][li + 1];
-      f.tyy[q] = s.yy[lj + 1][li + 1];
-      if (i < nx - 1 && j < ny - 1) f.txy[q] = s.xy[lj + 2][li + 2];
-    }
-  }
-  if (RECORD) {
-    for (int o = 16; o > 0; o >>= 1) {
-      vmx = fmax(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
-      vmy = fmax(vmy, __shfl_xor_sync(0xffffffffu, vmy, o));
-    }
-    if ((tid & 31) == 0) {
-      atomic_max_nonneg(&f.vmax[0], vmx);
-      atomic_max_nonneg(&f.vmax[1], vmy);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------
 // RVE averaging (EffPlast2D.cu:430-503) as a deterministic two-level reduction:
 // per-block partials in a fixed order, then one block sums the partials in order.
 // Sums: 0..3 sigma (sigma[3] stays 0 as in the reference), 4..7 sigmaPer, 8..10 epsPer.

@@ -1,0 +1,254 @@
+// ep2d_iter_f64.cuh -- the fused FP64 iteration kernel (north-star items a and b).
+//
+// One launch = one pseudo-time iteration of the reference's four kernels
+// ComputeStress (EffPlast2D.cu:37-98) -> ComputeJ2 (:100-145) -> ComputePlasticity
+// (:147-177) -> ComputeDisp (:3-35).  A CTA of 32 x 8 threads owns a TX x TY block of
+// nodes and of the faces with the same (i, j):
+//   A  stage Ux, Uy (halo 1-2) and the node mask in shared memory; the owned Vx, Vy are
+//      loaded into registers at the same time, so their latency hides behind A-C;
+//   B  trial stresses on the halo region: P, tauXX, tauYY at (TX+2) x (TY+2) nodes,
+//      tauXY at (TX+2) x (TY+2) corners, zeroed inside pores;
+//   C  (NL > 1) J2 radial return: nodes use tauXY averaged onto the node (the nine
+//      edge stencils of :109-135 are one clamped 2x2 corner block), corners use tauXX,
+//      tauYY averaged onto the corner, both from the pre-return values;
+//   D  damped momentum update and U += V dt on the owned faces, U written to the other
+//      ping-pong buffer.
+// Stresses stay on chip; RECORD launches (checkpoints, last iteration) also write the
+// stress fields and fold max|Vx|, max|Vy| into vmax (north-star item c).
+//
+// Arithmetic: divisions by dX, dY, 3 and rho are multiplications by reciprocals
+// computed once on the host, and the yield test compares J2^2 with coh^2 so that the
+// square root and the division by J2 run only in yielding cells.  Results differ from
+// the reference's division/sqrt forms by rounding only (parity tests: 1e-9).
+#pragma once
+
+#include "ep2d_types.hpp"
+
+namespace ep2d {
+
+template <int TX, int TY>
+struct TileSmem {
+  static constexpr int UW = TX + 3, UH = TY + 3;  // Ux, Uy, mask halo tiles
+  static constexpr int SW = TX + 2, SH = TY + 2;  // node stress and corner stress tiles
+  static constexpr int FW = TX + 1, FH = TY + 1;  // return factors
+  double ux[UH][UW];
+  double uy[UH][UW];
+  double p[SH][SW];
+  double xx[SH][SW];
+  double yy[SH][SW];
+  double xy[SH][SW];
+  double fn[FH][FW];
+  double fc[FH][FW];
+  uint8_t m[UH][UW];
+};
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int TX, int TY, bool PLASTIC, bool RECORD>
+__global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
+  static_assert(TX == 32 && TY % 8 == 0, "the thread mapping assumes 32 x 8 threads and TX == 32");
+  using S = TileSmem<TX, TY>;
+  constexpr int UW = S::UW, UH = S::UH, SW = S::SW, SH = S::SH, FW = S::FW, FH = S::FH;
+  constexpr int RY = TY / 8;  // owned rows per thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int nx = g.nx, ny = g.ny;
+  const size_t pitch = (size_t)g.pitch;
+  const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
+  const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
+  double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
+  double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
+
+  // owned velocities, fetched first
+  double vxr[RY], vyr[RY];
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int i = i0 + tx, j = j0 + ty + 8 * r;
+    const bool ok = (i < nx && j < ny);
+    vxr[r] = ok ? f.vx[j * pitch + i] : 0.0;
+    vyr[r] = ok ? f.vy[j * pitch + i] : 0.0;
+  }
+
+  // ---- A: stage Ux (i in [i0-1, i0+TX+1], j in [j0-2, j0+TY]), Uy (i in [i0-2, i0+TX],
+  //         j in [j0-1, j0+TY+1]) and the mask (nodes [i0-2, i0+TX] x [j0-2, j0+TY])
+#pragma unroll
+  for (int lj = ty; lj < UH; lj += 8) {
+#pragma unroll
+    for (int li = tx; li < UW; li += 32) {
+      int i = i0 - 1 + li, j = j0 - 2 + lj;
+      s.ux[lj][li] = (i >= 0 && i <= nx && j >= 0 && j < ny) ? ux[j * pitch + i] : 0.0;
+      i = i0 - 2 + li;
+      j = j0 - 1 + lj;
+      s.uy[lj][li] = (i >= 0 && i < nx && j >= 0 && j <= ny) ? uy[j * pitch + i] : 0.0;
+      j = j0 - 2 + lj;
+      s.m[lj][li] = (i >= 0 && i < nx && j >= 0 && j < ny) ? f.mask[j * pitch + i] : (uint8_t)0;
+    }
+  }
+  __syncthreads();
+
+  const double rdX = g.rdX, rdY = g.rdY;
+  const double third = 1.0 / 3.0;
+  // ---- B: trial stresses at nodes (i0-1+li, j0-1+lj) and corners (i0-2+li, j0-2+lj)
+#pragma unroll
+  for (int lj = ty; lj < SH; lj += 8) {
+#pragma unroll
+    for (int li = tx; li < SW; li += 32) {
+      {
+        const int i = i0 - 1 + li, j = j0 - 1 + lj;
+        double pv = 0.0, xv = 0.0, yv = 0.0;
+        if (i >= 0 && i < nx && j >= 0 && j < ny) {
+          const uint8_t m = s.m[lj + 1][li + 1];
+          const double K = (m & M_MAT) ? g.Kp : g.K0;
+          const double G2 = 2.0 * ((m & M_MAT) ? g.Gp : g.G0);
+          const double exx = (s.ux[lj + 1][li + 1] - s.ux[lj + 1][li]) * rdX;
+          const double eyy = (s.uy[lj + 1][li + 1] - s.uy[lj][li + 1]) * rdY;
+          const double divU = exx + eyy;
+          if (!(m & M_NODE)) {
+            pv = -K * divU;
+            xv = G2 * (exx - divU * third);
+            yv = G2 * (eyy - divU * third);
+          }
+        }
+        s.p[lj][li] = pv;
+        s.xx[lj][li] = xv;
+        s.yy[lj][li] = yv;
+      }
+      {
+        const int ci = i0 - 2 + li, cj = j0 - 2 + lj;
+        double t = 0.0;
+        if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
+          const uint8_t m00 = s.m[lj][li], m10 = s.m[lj][li + 1], m01 = s.m[lj + 1][li], m11 = s.m[lj + 1][li + 1];
+          if (!(m00 & M_CORNER)) {
+            const double Gs = ((m00 & M_MAT) ? g.Gp : g.G0) + ((m10 & M_MAT) ? g.Gp : g.G0) +
+                              ((m01 & M_MAT) ? g.Gp : g.G0) + ((m11 & M_MAT) ? g.Gp : g.G0);
+            t = 0.25 * Gs * ((s.ux[lj + 1][li] - s.ux[lj][li]) * rdY + (s.uy[lj][li + 1] - s.uy[lj][li]) * rdX);
+          }
+        }
+        s.xy[lj][li] = t;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- C: J2 radial return (NL > 1, EffPlast2D.cu:392-397)
+  if (PLASTIC) {
+    const double coh = g.coh, coh2 = g.coh2;
+#pragma unroll
+    for (int lj = ty; lj < FH; lj += 8) {
+#pragma unroll
+      for (int li = tx; li < FW; li += 32) {
+        {  // node (i0-1+li, j0-1+lj)
+          const int i = i0 - 1 + li, j = j0 - 1 + lj;
+          double fn = 1.0;
+          if (i >= 0 && i < nx && j >= 0 && j < ny) {
+            const int a = min(max(i - 1, 0), nx - 3) - (i0 - 2), b = min(max(j - 1, 0), ny - 3) - (j0 - 2);
+            const double tav = 0.25 * (s.xy[b][a] + s.xy[b][a + 1] + s.xy[b + 1][a] + s.xy[b + 1][a + 1]);
+            const double xv = s.xx[lj][li], yv = s.yy[lj][li];
+            const double J2sq = xv * xv + yv * yv + 2.0 * tav * tav;
+            double J2 = 0.0;
+            if (J2sq > coh2) {
+              J2 = sqrt(J2sq);
+              fn = coh / J2;
+            }
+            if (RECORD && li >= 1 && lj >= 1) {
+              double tavo = tav, J2o = (J2sq > coh2) ? J2 : sqrt(J2sq);
+              if (fn != 1.0) {
+                const double xo = xv * fn, yo = yv * fn;
+                tavo = tav * fn;
+                J2o = sqrt(xo * xo + yo * yo + 2.0 * tavo * tavo);
+              }
+              f.txyav[j * pitch + i] = tavo;
+              f.j2[j * pitch + i] = J2o;
+            }
+          }
+          s.fn[lj][li] = fn;
+        }
+        {  // corner (i0-1+li, j0-1+lj)
+          const int ci = i0 - 1 + li, cj = j0 - 1 + lj;
+          double fc = 1.0;
+          if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
+            const double sx = s.xx[lj][li] + s.xx[lj][li + 1] + s.xx[lj + 1][li] + s.xx[lj + 1][li + 1];
+            const double sy = s.yy[lj][li] + s.yy[lj][li + 1] + s.yy[lj + 1][li] + s.yy[lj + 1][li + 1];
+            const double t = s.xy[lj + 1][li + 1];
+            const double J2sq = 0.0625 * sx * sx + 0.0625 * sy * sy + 2.0 * t * t;
+            if (J2sq > coh2) fc = coh / sqrt(J2sq);
+            if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = sqrt(J2sq);
+          }
+          s.fc[lj][li] = fc;
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int lj = ty; lj < FH; lj += 8) {
+#pragma unroll
+      for (int li = tx; li < FW; li += 32) {
+        const double fn = s.fn[lj][li];
+        s.xx[lj][li] *= fn;
+        s.yy[lj][li] *= fn;
+        s.xy[lj + 1][li + 1] *= s.fc[lj][li];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- D: damped momentum update and U += V dt on the owned faces
+  const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
+  double vmx = 0.0, vmy = 0.0;
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int li = tx, lj = ty + 8 * r;
+    const int i = i0 + li, j = j0 + lj;
+    if (i >= nx || j >= ny) continue;
+    const size_t q = j * pitch + i;
+    double vx = vxr[r];
+    if (i > 0 && j > 0 && j < ny - 1) {
+      vx = vx * cX + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj + 1][li] + s.xx[lj + 1][li + 1] - s.xx[lj + 1][li]) * rdX +
+                            (s.xy[lj + 2][li + 1] - s.xy[lj + 1][li + 1]) * rdY);
+      f.vx[q] = vx;
+    }
+    uxo[q] = s.ux[lj + 2][li + 1] + vx * dT;
+    double vy = vyr[r];
+    if (i > 0 && i < nx - 1 && j > 0) {
+      vy = vy * cY + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj][li + 1] + s.yy[lj + 1][li + 1] - s.yy[lj][li + 1]) * rdY +
+                            (s.xy[lj + 1][li + 2] - s.xy[lj + 1][li + 1]) * rdX);
+      f.vy[q] = vy;
+    }
+    uyo[q] = s.uy[lj + 1][li + 2] + vy * dT;
+    if (i == nx - 1) {  // face column i = nx of Ux/Vx: never updated by the reference
+      const size_t q2 = j * pitch + nx;
+      uxo[q2] = s.ux[lj + 2][li + 2];
+      if (RECORD) vmx = fmax(vmx, fabs(f.vx[q2]));
+    }
+    if (j == ny - 1) {  // face row j = ny of Uy/Vy
+      const size_t q3 = (size_t)ny * pitch + i;
+      uyo[q3] = s.uy[lj + 2][li + 2];
+      if (RECORD) vmy = fmax(vmy, fabs(f.vy[q3]));
+    }
+    if (RECORD) {
+      vmx = fmax(vmx, fabs(vx));
+      vmy = fmax(vmy, fabs(vy));
+      f.p[q] = s.p[lj + 1][li + 1];
+      f.txx[q] = s.xx[lj + 1][li + 1];
+      f.tyy[q] = s.yy[lj + 1][li + 1];
+      if (i < nx - 1 && j < ny - 1) f.txy[q] = s.xy[lj + 2][li + 2];
+    }
+  }
+  if (RECORD) {
+    for (int o = 16; o > 0; o >>= 1) {
+      vmx = fmax(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
+      vmy = fmax(vmy, __shfl_xor_sync(0xffffffffu, vmy, o));
+    }
+    if (tx == 0) {
+      atomic_max_nonneg(&f.vmax[0], vmx);
+      atomic_max_nonneg(&f.vmax[1], vmy);
+    }
+  }
+}
+
+}  // namespace ep2d

@@ -1,5 +1,6 @@
 // ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh.
 #include "ep2d_device.cuh"
+#include "ep2d_iter_f64.cuh"
 
 namespace ep2d {
 

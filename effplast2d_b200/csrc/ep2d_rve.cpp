@@ -354,6 +354,12 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   g.Gp = 0.01 * g.G0;
   g.rad = p.pa[9];
   g.nPores = p.pa[10];
+  g.rdX = 1.0 / g.dX;
+  g.rdY = 1.0 / g.dY;
+  g.coh2 = g.coh * g.coh;
+  g.cX = 1.0 - g.dT * g.dampX;
+  g.cY = 1.0 - g.dT * g.dampY;
+  g.dtr = g.dT / g.rho;
 
   if (s) {
     stream = s;

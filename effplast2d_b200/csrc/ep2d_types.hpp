@@ -16,6 +16,9 @@ struct Geo {
   double dX, dY, dT, rho, dampX, dampY, coh;
   double K0, G0, Kp, Gp;  // Kp = 0.01 * K0, Gp = 0.01 * G0 (EffPlast2D.cu:721-722)
   double rad, nPores;
+  // host-computed factors of the iteration kernel: 1/dX, 1/dY, coh^2,
+  // 1 - dT dampX, 1 - dT dampY, dT / rho
+  double rdX, rdY, coh2, cX, cY, dtr;
 };
 
 // Device pointers of one RVE on the FP64 path.
