@@ -107,8 +107,67 @@ class Result(ctypes.Structure):
         }
 
 
+class RveSpec(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32),
+        ("pa", c_double * NPARS),
+        ("nl", c_int32), ("n_time_steps", c_int32),
+        ("init_load_value", c_double),
+        ("load_type", c_double * 3),
+    ]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("niter", c_int64), ("eiter", c_double),
+        ("check_every", c_int32), ("precision", c_int32), ("device", c_int32),
+        ("tile_y", c_int32), ("graph_len", c_int32), ("reserved", c_int32),
+    ]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("kernel_ms", c_double), ("wall_ms", c_double),
+        ("launches", c_int64), ("all_launches", c_int64), ("cell_updates", c_int64),
+        ("tile_y", c_int32), ("blocks", c_int32),
+        ("tune_us", c_double * 3),
+    ]
+
+    def as_dict(self):
+        return {"kernel_ms": self.kernel_ms, "wall_ms": self.wall_ms, "launches": self.launches,
+                "all_launches": self.all_launches, "cell_updates": self.cell_updates,
+                "tile_y": self.tile_y, "blocks": self.blocks, "tune_us": list(self.tune_us)}
+
+
+def make_spec(nx, ny, pa, nl, n_time_steps, init_load_value, load_type):
+    s = RveSpec()
+    s.nx, s.ny = int(nx), int(ny)
+    for i, v in enumerate(pa):
+        s.pa[i] = float(v)
+    s.nl = int(nl)
+    s.n_time_steps = int(n_time_steps)
+    s.init_load_value = float(init_load_value)
+    for i in range(3):
+        s.load_type[i] = float(load_type[i])
+    return s
+
+
+def make_batch_config(niter=100000, eiter=1e-9, check_every=10000, precision=FP64, device=0, tile_y=0,
+                      graph_len=0):
+    c = BatchConfig()
+    c.niter = int(niter)
+    c.eiter = float(eiter)
+    c.check_every = int(check_every)
+    c.precision = int(precision)
+    c.device = int(device)
+    c.tile_y = int(tile_y)
+    c.graph_len = int(graph_len)
+    return c
+
+
 STRUCTS = {"ep2d_params": Params, "ep2d_step_record": StepRecord,
-           "ep2d_moduli": Moduli, "ep2d_result": Result}
+           "ep2d_moduli": Moduli, "ep2d_result": Result, "ep2d_rve_spec": RveSpec,
+           "ep2d_batch_config": BatchConfig, "ep2d_batch_stats": BatchStats}
 
 
 def make_params(nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000,

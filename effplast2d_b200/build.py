@@ -20,8 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_INC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
 
 CU_SOURCES = ["ep2d_kernels.cu"]
-CPP_SOURCES = ["ep2d_rve.cpp", "ep2d_api.cpp"]
-HEADERS = ["ep2d_device.cuh", "ep2d_iter_f64.cuh", "ep2d_types.hpp", "ep2d_rve.hpp"]
+CPP_SOURCES = ["ep2d_rve.cpp", "ep2d_api.cpp", "ep2d_batch.cpp"]
+HEADERS = ["ep2d_device.cuh", "ep2d_iter_f64.cuh", "ep2d_types.hpp", "ep2d_rve.hpp", "ep2d_batch.hpp"]
 
 
 def _newer(target, deps):

@@ -85,8 +85,6 @@ int ep2d_create(const ep2d_params* params, ep2d_handle** out) {
   if (!params || !out) return fail(EP2D_ERR_ARG, "null argument");
   *out = nullptr;
   EP2D_GUARD({
-    if (params->precision != EP2D_FP64)
-      return fail(EP2D_ERR_ARG, "single-RVE handles run the FP64 path; use the batch API for EP2D_MIXED");
     ep2d_handle* h = new ep2d_handle();
     int rc = h->rve.create(*params);
     if (rc) {
@@ -195,10 +193,12 @@ int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t
 
 // sizeof() of every ABI struct, for the binding's layout check
 int ep2d_abi_sizes(int64_t* out, int32_t n) {
-  const int64_t s[4] = {(int64_t)sizeof(ep2d_params), (int64_t)sizeof(ep2d_step_record),
-                        (int64_t)sizeof(ep2d_moduli), (int64_t)sizeof(ep2d_result)};
-  for (int32_t k = 0; k < n && k < 4; k++) out[k] = s[k];
-  return 4;
+  const int64_t s[7] = {(int64_t)sizeof(ep2d_params),      (int64_t)sizeof(ep2d_step_record),
+                        (int64_t)sizeof(ep2d_moduli),      (int64_t)sizeof(ep2d_result),
+                        (int64_t)sizeof(ep2d_rve_spec),    (int64_t)sizeof(ep2d_batch_config),
+                        (int64_t)sizeof(ep2d_batch_stats)};
+  for (int32_t k = 0; k < n && k < 7; k++) out[k] = s[k];
+  return 7;
 }
 
 }  // extern "C"

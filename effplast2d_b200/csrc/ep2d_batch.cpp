@@ -1,0 +1,671 @@
+// ep2d_batch.cpp -- batched persistent solver and continuous-batching server.
+#include "ep2d_batch.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+
+namespace ep2d {
+
+#define EP2D_CK(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+ep2d_params params_of(const ep2d_batch_config& c, const ep2d_rve_spec& s) {
+  ep2d_params p{};
+  p.nx = s.nx;
+  p.ny = s.ny;
+  std::memcpy(p.pa, s.pa, sizeof(p.pa));
+  p.nl = s.nl;
+  p.check_every = c.check_every;
+  p.niter = c.niter;
+  p.eiter = c.eiter;
+  p.precision = c.precision;
+  p.device = c.device;
+  return p;
+}
+
+int validate_config(const ep2d_batch_config& c) {
+  if (c.check_every < 2) return fail(EP2D_ERR_ARG, "check_every must be >= 2 in a batch");
+  if (c.niter < c.check_every || c.niter % c.check_every != 0)
+    return fail(EP2D_ERR_ARG, "niter must be a positive multiple of check_every in a batch");
+  if (c.precision != EP2D_FP64 && c.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
+  if (c.tile_y != 0 && c.tile_y != 8 && c.tile_y != 16 && c.tile_y != 32)
+    return fail(EP2D_ERR_ARG, "tile_y must be 0, 8, 16 or 32");
+  if (c.graph_len < 0 || (c.graph_len % 2) != 0) return fail(EP2D_ERR_ARG, "graph_len must be even");
+  return EP2D_OK;
+}
+}  // namespace
+
+BatchEngine::~BatchEngine() {
+  if (!stream) return;
+  DeviceScope ds(device);
+  cudaStreamSynchronize(stream);
+  slots_.clear();
+  if (graph_) cudaGraphExecDestroy(graph_);
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  cudaFree(d_ents_);
+  cudaFree(d_tiles_);
+  cudaFree(d_ntiles_);
+  cudaFree(d_vmax_);
+  if (h_vmax_) cudaFreeHost(h_vmax_);
+  cudaStreamDestroy(stream);
+}
+
+int BatchEngine::init(const ep2d_batch_config& c) {
+  int rc = validate_config(c);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(EP2D_ERR_NODEV, "no CUDA device");
+  }
+  if (c.device < 0 || c.device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");
+  cfg = c;
+  if (cfg.graph_len == 0) cfg.graph_len = 64;
+  device = c.device;
+  DeviceScope ds(device);
+  rc = prepare_device(device);
+  if (rc) return rc;
+  EP2D_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device));
+  EP2D_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  EP2D_CK(cudaEventCreate(&ev_[0]));
+  EP2D_CK(cudaEventCreate(&ev_[1]));
+  EP2D_CK(cudaMalloc(&d_ntiles_, sizeof(int)));
+  tile_y = c.tile_y ? c.tile_y : TILE_Y;
+  tuned = c.tile_y != 0;
+  blocks = sm_count_ * iter_blocks_per_sm(false, c.precision == EP2D_MIXED, tile_y);
+  return grow(16);
+}
+
+size_t BatchEngine::footprint(const ep2d_rve_spec& s) const { return Rve::footprint(params_of(cfg, s)); }
+
+int BatchEngine::grow(int need) {
+  if (need <= cap_slots_) return EP2D_OK;
+  const int cap = std::max(need, 2 * cap_slots_);
+  DeviceScope ds(device);
+  EP2D_CK(cudaStreamSynchronize(stream));
+  cudaFree(d_ents_);
+  cudaFree(d_vmax_);
+  if (h_vmax_) cudaFreeHost(h_vmax_);
+  d_ents_ = nullptr;
+  d_vmax_ = nullptr;
+  h_vmax_ = nullptr;
+  EP2D_CK(cudaMalloc(&d_ents_, cap * sizeof(BatchEntry)));
+  EP2D_CK(cudaMalloc(&d_vmax_, cap * 2 * sizeof(unsigned long long)));
+  EP2D_CK(cudaMallocHost(&h_vmax_, cap * 2 * sizeof(unsigned long long)));
+  cap_slots_ = cap;
+  if (graph_) {  // the graph holds the old pointers
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  tiles_dirty_ = true;
+  return EP2D_OK;
+}
+
+int BatchEngine::active() const {
+  int n = 0;
+  for (const auto& s : slots_) n += (s.used && !s.task.done) ? 1 : 0;
+  return n;
+}
+
+int BatchEngine::begin_task_step(Slot& s) {
+  Task& t = s.task;
+  double lsv, lt[3];
+  int nts;
+  Rve::step_load(t.step, t.spec.init_load_value, t.spec.load_type, t.spec.n_time_steps, &lsv, lt, &nts);
+  if (t.it == 0) {
+    const int rc = s.rve->begin_step(t.step, nts);
+    if (rc) return rc;
+  }
+  t.iters = 0;
+  const int rc = s.rve->begin_time_step(t.step, t.it, lsv, lt, nts);
+  aux_launches += 1;
+  return rc;
+}
+
+int BatchEngine::add(const ep2d_rve_spec& spec, uint64_t ticket, double submit_s, int* slot_out) {
+  DeviceScope ds(device);
+  if (spec.n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
+  int slot = -1;
+  for (size_t k = 0; k < slots_.size(); k++)
+    if (!slots_[k].used) {
+      slot = (int)k;
+      break;
+    }
+  if (slot < 0) {
+    slot = (int)slots_.size();
+    slots_.emplace_back();
+  }
+  int rc = grow((int)slots_.size());
+  if (rc) return rc;
+  Slot& s = slots_[slot];
+  s.rve.reset(new Rve());
+  rc = s.rve->create(params_of(cfg, spec), stream);
+  if (rc) {
+    s.rve.reset();
+    return rc;
+  }
+  s.rve->tile_y = tile_y;
+  s.used = true;
+  s.task = Task{};
+  s.task.spec = spec;
+  s.task.ticket = ticket;
+  s.task.submit_s = submit_s;
+  s.task.admit_s = now_s();
+  s.rve->begin_chain(spec.load_type);
+  rc = begin_task_step(s);
+  if (rc) {
+    s.rve.reset();
+    s.used = false;
+    return rc;
+  }
+  bytes_ += footprint(spec);
+  tiles_dirty_ = true;
+  if (slot_out) *slot_out = slot;
+  return EP2D_OK;
+}
+
+int BatchEngine::rebuild_tiles() {
+  std::vector<int2> tiles;
+  for (size_t k = 0; k < slots_.size(); k++) {
+    const Slot& s = slots_[k];
+    if (!s.used || s.task.done) continue;
+    const int tx = (s.rve->g.nx + TILE_X - 1) / TILE_X, ty = (s.rve->g.ny + tile_y - 1) / tile_y;
+    for (int by = 0; by < ty; by++)
+      for (int bx = 0; bx < tx; bx++) tiles.push_back(make_int2((int)k, bx | (by << 16)));
+  }
+  if ((int)tiles.size() > cap_tiles_) {
+    const int cap = std::max((int)tiles.size(), 2 * cap_tiles_);
+    EP2D_CK(cudaStreamSynchronize(stream));
+    cudaFree(d_tiles_);
+    d_tiles_ = nullptr;
+    EP2D_CK(cudaMalloc(&d_tiles_, (size_t)cap * sizeof(int2)));
+    cap_tiles_ = cap;
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+  }
+  n_tiles_ = (int)tiles.size();
+  if (n_tiles_)
+    EP2D_CK(cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, stream));
+  EP2D_CK(cudaMemcpyAsync(d_ntiles_, &n_tiles_, sizeof(int), cudaMemcpyHostToDevice, stream));
+  EP2D_CK(cudaStreamSynchronize(stream));  // the host vectors go out of scope
+  tiles_dirty_ = false;
+  return EP2D_OK;
+}
+
+int BatchEngine::ensure_graph() {
+  if (graph_ && graph_tile_y_ == tile_y) return EP2D_OK;
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  const bool mixed = cfg.precision == EP2D_MIXED;
+  cudaGraph_t g = nullptr;
+  EP2D_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t le = cudaSuccess;
+  for (int k = 0; k < cfg.graph_len && le == cudaSuccess; k++)
+    le = launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, k & 1, false, mixed, tile_y, blocks, stream);
+  const cudaError_t ee = cudaStreamEndCapture(stream, &g);
+  if (le != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(EP2D_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&graph_, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+  graph_tile_y_ = tile_y;
+  return EP2D_OK;
+}
+
+// launches k0 .. k0+n-1 of the interval (parity k & 1), graphs where aligned
+int BatchEngine::launch_plain_run(int64_t k0, int64_t n) {
+  const bool mixed = cfg.precision == EP2D_MIXED;
+  int64_t k = k0;
+  while (n > 0) {
+    if ((k & 1) == 0 && n >= cfg.graph_len && graph_) {
+      EP2D_CK(cudaGraphLaunch(graph_, stream));
+      k += cfg.graph_len;
+      n -= cfg.graph_len;
+    } else {
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(k & 1), false, mixed, tile_y, blocks, stream));
+      k++;
+      n--;
+    }
+  }
+  return EP2D_OK;
+}
+
+// Time the tile heights on real iterations of the first interval (they advance the
+// solution like any other launch) and keep the fastest.  *k: launches done so far.
+int BatchEngine::autotune(int64_t* k, int64_t n_avail) {
+  const int cand[3] = {16, 8, 32};
+  const int per = 24;  // 4 warm-up + 20 timed launches per candidate
+  if (n_avail < 3 * per) {
+    tuned = true;
+    return EP2D_OK;
+  }
+  const bool mixed = cfg.precision == EP2D_MIXED;
+  float best = 1e30f;
+  int best_ty = tile_y;
+  for (int c = 0; c < 3; c++) {
+    tile_y = cand[c];
+    blocks = sm_count_ * iter_blocks_per_sm(false, mixed, tile_y);
+    int rc = rebuild_tiles();
+    if (rc) return rc;
+    for (int w = 0; w < 4; w++, (*k)++)
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, tile_y, blocks, stream));
+    EP2D_CK(cudaEventRecord(ev_[0], stream));
+    for (int w = 0; w < per - 4; w++, (*k)++)
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, tile_y, blocks, stream));
+    EP2D_CK(cudaEventRecord(ev_[1], stream));
+    EP2D_CK(cudaEventSynchronize(ev_[1]));
+    float ms = 0.0f;
+    EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    kernel_ms += ms;
+    const float us = 1000.0f * ms / (per - 4);
+    tune_us[tile_y == 8 ? 0 : (tile_y == 16 ? 1 : 2)] = us;
+    if (us < best) {
+      best = us;
+      best_ty = tile_y;
+    }
+  }
+  tile_y = best_ty;
+  blocks = sm_count_ * iter_blocks_per_sm(false, mixed, tile_y);
+  for (auto& s : slots_)
+    if (s.used) s.rve->tile_y = tile_y;
+  tuned = true;
+  return rebuild_tiles();
+}
+
+int BatchEngine::advance(Slot& s, double error) {
+  Task& t = s.task;
+  Rve& r = *s.rve;
+  ep2d_step_record& rec = r.rec[t.step][t.it];
+  r.checks[t.step][t.it].push_back(error);
+  rec.n_checks++;
+  const bool conv = error < cfg.eiter;
+  if (!conv && t.iters < cfg.niter) return EP2D_OK;  // keep iterating
+  rec.iterations = conv ? t.iters : cfg.niter;
+  rec.converged = conv ? 1 : 0;
+  rec.error = error;
+  int rc = r.finish_time_step(t.step, t.it);
+  aux_launches += 4;
+  if (rc) return rc;
+  if (t.it + 1 < r.nts[t.step]) {
+    t.it++;
+    return begin_task_step(s);
+  }
+  if (t.step + 1 < r.prm.nl) {
+    t.step++;
+    t.it = 0;
+    return begin_task_step(s);
+  }
+  r.finish_chain(t.spec.n_time_steps, &t.result);
+  t.done = true;
+  t.done_s = now_s();
+  finished_.push_back(t);
+  bytes_ -= footprint(t.spec);
+  s.rve.reset();  // release the RVE's device memory
+  s.used = false;
+  tiles_dirty_ = true;
+  return EP2D_OK;
+}
+
+int BatchEngine::run_interval() {
+  if (active() == 0) return EP2D_OK;
+  DeviceScope ds(device);
+  const bool mixed = cfg.precision == EP2D_MIXED;
+  // entries: geometry, pointers, current ping-pong parity, per-slot vmax
+  std::vector<BatchEntry> ents(slots_.size());
+  int64_t cells = 0;
+  for (size_t k = 0; k < slots_.size(); k++) {
+    Slot& s = slots_[k];
+    if (!s.used) continue;
+    s.rve->f.vmax = d_vmax_ + 2 * k;
+    ents[k].g = s.rve->g;
+    ents[k].f = s.rve->f;
+    ents[k].src0 = s.rve->cur;
+    ents[k].plastic = s.rve->prm.nl > 1 ? 1 : 0;
+    cells += (int64_t)s.rve->g.nx * s.rve->g.ny;
+  }
+  EP2D_CK(cudaMemcpyAsync(d_ents_, ents.data(), ents.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, stream));
+  if (tiles_dirty_) {
+    const int rc = rebuild_tiles();
+    if (rc) return rc;
+  } else {
+    EP2D_CK(cudaStreamSynchronize(stream));
+  }
+  const int64_t ce = cfg.check_every;
+  int64_t k = 0;
+  if (!tuned) {
+    const int rc = autotune(&k, ce - 1);
+    if (rc) return rc;
+  }
+  int rc = ensure_graph();
+  if (rc) return rc;
+  EP2D_CK(cudaEventRecord(ev_[0], stream));
+  rc = launch_plain_run(k, ce - 1 - k);
+  if (rc) return rc;
+  EP2D_CK(cudaMemsetAsync(d_vmax_, 0, slots_.size() * 2 * sizeof(unsigned long long), stream));
+  EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)((ce - 1) & 1), true, mixed, tile_y, blocks, stream));
+  EP2D_CK(cudaEventRecord(ev_[1], stream));
+  EP2D_CK(cudaMemcpyAsync(h_vmax_, d_vmax_, slots_.size() * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          stream));
+  EP2D_CK(cudaStreamSynchronize(stream));
+  float ms = 0.0f;
+  EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+  kernel_ms += ms;
+  launches += ce;
+  cell_updates += ce * cells;
+  for (size_t q = 0; q < slots_.size(); q++) {
+    Slot& s = slots_[q];
+    if (!s.used || s.task.done) continue;
+    s.rve->cur ^= (int)(ce & 1);
+    s.task.iters += ce;
+    double vmx, vmy;
+    std::memcpy(&vmx, &h_vmax_[2 * q], sizeof(double));
+    std::memcpy(&vmy, &h_vmax_[2 * q + 1], sizeof(double));
+    rc = advance(s, s.rve->error_from_vmax(vmx, vmy));
+    if (rc) {
+      s.task.status = rc;
+      s.task.done = true;
+      s.task.done_s = now_s();
+      finished_.push_back(s.task);
+      bytes_ -= footprint(s.task.spec);
+      s.rve.reset();
+      s.used = false;
+      tiles_dirty_ = true;
+    }
+  }
+  return EP2D_OK;
+}
+
+std::vector<Task> BatchEngine::take_finished() {
+  std::vector<Task> out;
+  out.swap(finished_);
+  return out;
+}
+
+// ---- server -------------------------------------------------------------------------
+class Server {
+ public:
+  int start(const ep2d_batch_config& c, int64_t budget, int32_t max_active) {
+    budget_ = budget;
+    max_active_ = max_active > 0 ? max_active : 1 << 30;
+    std::unique_lock<std::mutex> lk(mu_);
+    worker_ = std::thread([this, c] { loop(c); });
+    cv_.wait(lk, [this] { return started_; });
+    return init_rc_;
+  }
+  void stop() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+  }
+  int submit(const ep2d_rve_spec& s, uint64_t* ticket) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!init_ok_) return fail(EP2D_ERR_STATE, "server is not running");
+    Task t;
+    t.spec = s;
+    t.ticket = ++next_ticket_;
+    t.submit_s = now_s();
+    pending_.push_back(t);
+    submitted_++;
+    if (ticket) *ticket = t.ticket;
+    cv_.notify_all();
+    return EP2D_OK;
+  }
+  int wait(uint64_t ticket, int32_t timeout_ms, int32_t* done, ep2d_result* res, double* lat, double* queue) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto ready = [&] { return done_.count(ticket) > 0 || !init_ok_; };
+    if (timeout_ms < 0) cv_.wait(lk, ready);
+    else cv_.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+    auto it = done_.find(ticket);
+    if (it == done_.end()) {
+      if (done) *done = 0;
+      return init_ok_ ? EP2D_OK : fail(EP2D_ERR_STATE, "server stopped");
+    }
+    if (done) *done = 1;
+    if (res) *res = it->second.result;
+    if (lat) *lat = it->second.done_s - it->second.submit_s;
+    if (queue) *queue = it->second.admit_s - it->second.submit_s;
+    const int st = it->second.status;
+    return st == EP2D_OK ? EP2D_OK : fail(st, "request failed");
+  }
+  void stats(int64_t* sub, int64_t* adm, int64_t* fin, int64_t* bytes, ep2d_batch_stats* es) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (sub) *sub = submitted_;
+    if (adm) *adm = admitted_;
+    if (fin) *fin = finished_;
+    if (bytes) *bytes = (int64_t)bytes_snapshot_;
+    if (es) *es = stats_snapshot_;
+  }
+
+ private:
+  void loop(ep2d_batch_config c) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      init_rc_ = eng_.init(c);
+      init_ok_ = init_rc_ == EP2D_OK;
+      started_ = true;
+      if (!init_ok_) init_msg_ = last_error();
+    }
+    cv_.notify_all();
+    if (!init_ok_) return;
+    while (true) {
+      std::vector<Task> admit;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || !pending_.empty() || !eng_.idle(); });
+        if (stop_) break;
+        size_t bytes = eng_.bytes_in_use();
+        int act = eng_.active();
+        while (!pending_.empty() && act < max_active_) {
+          const size_t need = eng_.footprint(pending_.front().spec);
+          if ((int64_t)(bytes + need) > budget_ && act > 0) break;  // wait for memory to free up
+          admit.push_back(pending_.front());
+          pending_.pop_front();
+          bytes += need;
+          act++;
+        }
+      }
+      for (auto& t : admit) {
+        const int rc = eng_.add(t.spec, t.ticket, t.submit_s, nullptr);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (rc) {
+          t.status = rc;
+          t.done = true;
+          t.admit_s = t.done_s = now_s();
+          done_[t.ticket] = t;
+          finished_++;
+        } else {
+          admitted_++;
+        }
+      }
+      if (!eng_.idle()) {
+        const int rc = eng_.run_interval();
+        (void)rc;
+      }
+      std::vector<Task> fin = eng_.take_finished();
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto& t : fin) {
+          done_[t.ticket] = t;
+          finished_++;
+        }
+        bytes_snapshot_ = eng_.bytes_in_use();
+        stats_snapshot_.kernel_ms = eng_.kernel_ms;
+        stats_snapshot_.launches = eng_.launches;
+        stats_snapshot_.all_launches = eng_.launches + eng_.aux_launches;
+        stats_snapshot_.cell_updates = eng_.cell_updates;
+        stats_snapshot_.tile_y = eng_.tile_y;
+        stats_snapshot_.blocks = eng_.blocks;
+        for (int q = 0; q < 3; q++) stats_snapshot_.tune_us[q] = eng_.tune_us[q];
+      }
+      if (!fin.empty()) cv_.notify_all();
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    init_ok_ = false;
+    cv_.notify_all();
+  }
+
+  BatchEngine eng_;
+  std::thread worker_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<Task> pending_;
+  std::map<uint64_t, Task> done_;
+  uint64_t next_ticket_ = 0;
+  int64_t budget_ = 0;
+  int max_active_ = 0;
+  int64_t submitted_ = 0, admitted_ = 0, finished_ = 0;
+  size_t bytes_snapshot_ = 0;
+  ep2d_batch_stats stats_snapshot_{};
+  bool started_ = false, init_ok_ = false, stop_ = false;
+  int init_rc_ = EP2D_OK;
+  std::string init_msg_;
+};
+
+}  // namespace ep2d
+
+using ep2d::fail;
+
+struct ep2d_server {
+  ep2d::Server srv;
+};
+
+extern "C" {
+
+int64_t ep2d_rve_footprint(const ep2d_rve_spec* spec, int32_t precision) {
+  if (!spec) return -1;
+  ep2d_batch_config c{};
+  c.check_every = 2;
+  c.niter = 2;
+  c.precision = precision;
+  return (int64_t)ep2d::Rve::footprint(ep2d::params_of(c, *spec));
+}
+
+int ep2d_batch_solve(const ep2d_batch_config* cfg, const ep2d_rve_spec* specs, int32_t n, ep2d_result* results,
+                     ep2d_batch_stats* stats) {
+  if (!cfg || (!specs && n > 0) || n < 0) return fail(EP2D_ERR_ARG, "null argument");
+  try {
+    const double t0 = ep2d::now_s();
+    ep2d::BatchEngine eng;
+    int rc = eng.init(*cfg);
+    if (rc) return rc;
+    size_t need = 0;
+    for (int k = 0; k < n; k++) {
+      rc = ep2d::validate_params(ep2d::params_of(*cfg, specs[k]));
+      if (rc) return rc;
+      need += eng.footprint(specs[k]);
+    }
+    size_t free_b = 0, total_b = 0;
+    {
+      ep2d::DeviceScope ds(cfg->device);
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need > free_b)
+        return fail(EP2D_ERR_NOMEM, "the batch needs " + std::to_string(need) + " bytes, " + std::to_string(free_b) +
+                                        " are free; use the server for progressive admission");
+    }
+    for (int k = 0; k < n; k++) {
+      rc = eng.add(specs[k], (uint64_t)k, t0, nullptr);
+      if (rc) return rc;
+    }
+    std::vector<ep2d::Task> done;
+    while (!eng.idle()) {
+      rc = eng.run_interval();
+      if (rc) return rc;
+      for (auto& t : eng.take_finished()) done.push_back(t);
+    }
+    for (auto& t : eng.take_finished()) done.push_back(t);
+    int status = EP2D_OK;
+    for (auto& t : done) {
+      if (results) results[t.ticket] = t.result;
+      if (t.status && !status) status = t.status;
+    }
+    if (stats) {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->kernel_ms = eng.kernel_ms;
+      stats->wall_ms = 1000.0 * (ep2d::now_s() - t0);
+      stats->launches = eng.launches;
+      stats->all_launches = eng.launches + eng.aux_launches;
+      stats->cell_updates = eng.cell_updates;
+      stats->tile_y = eng.tile_y;
+      stats->blocks = eng.blocks;
+      for (int q = 0; q < 3; q++) stats->tune_us[q] = eng.tune_us[q];
+    }
+    return status ? fail(status, "a batch member failed") : EP2D_OK;
+  } catch (const std::exception& ex) {
+    return fail(EP2D_ERR_STATE, std::string("exception: ") + ex.what());
+  }
+}
+
+int ep2d_server_create(const ep2d_batch_config* cfg, int64_t mem_budget_bytes, int32_t max_active, ep2d_server** out) {
+  if (!cfg || !out) return fail(EP2D_ERR_ARG, "null argument");
+  *out = nullptr;
+  try {
+    ep2d_server* s = new ep2d_server();
+    const int rc = s->srv.start(*cfg, mem_budget_bytes, max_active);
+    if (rc) {
+      s->srv.stop();
+      delete s;
+      return rc;
+    }
+    *out = s;
+    return EP2D_OK;
+  } catch (const std::exception& ex) {
+    return fail(EP2D_ERR_STATE, std::string("exception: ") + ex.what());
+  }
+}
+
+int ep2d_server_submit(ep2d_server* s, const ep2d_rve_spec* spec, uint64_t* ticket_out) {
+  if (!s || !spec) return fail(EP2D_ERR_ARG, "null argument");
+  const int rc = ep2d::validate_params([&] {
+    ep2d_batch_config c{};
+    c.check_every = 2;
+    c.niter = 2;
+    return ep2d::params_of(c, *spec);
+  }());
+  if (rc) return rc;
+  return s->srv.submit(*spec, ticket_out);
+}
+
+int ep2d_server_wait(ep2d_server* s, uint64_t ticket, int32_t timeout_ms, int32_t* done, ep2d_result* result,
+                     double* latency_s, double* queue_s) {
+  if (!s) return fail(EP2D_ERR_ARG, "null server");
+  return s->srv.wait(ticket, timeout_ms, done, result, latency_s, queue_s);
+}
+
+int ep2d_server_stats(ep2d_server* s, int64_t* submitted, int64_t* admitted, int64_t* finished, int64_t* bytes_in_use,
+                      ep2d_batch_stats* engine) {
+  if (!s) return fail(EP2D_ERR_ARG, "null server");
+  s->srv.stats(submitted, admitted, finished, bytes_in_use, engine);
+  return EP2D_OK;
+}
+
+int ep2d_server_destroy(ep2d_server* s) {
+  if (!s) return EP2D_OK;
+  s->srv.stop();
+  delete s;
+  return EP2D_OK;
+}
+
+}  // extern "C"

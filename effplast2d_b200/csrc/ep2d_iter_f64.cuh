@@ -1,4 +1,5 @@
-// ep2d_iter_f64.cuh -- the fused FP64 iteration kernel (north-star items a and b).
+// ep2d_iter_f64.cuh -- the fused iteration kernel (north-star items a and b), single
+// RVE and batched.
 //
 // One launch = one pseudo-time iteration of the reference's four kernels
 // ComputeStress (EffPlast2D.cu:37-98) -> ComputeJ2 (:100-145) -> ComputePlasticity
@@ -16,10 +17,13 @@
 // Stresses stay on chip; RECORD launches (checkpoints, last iteration) also write the
 // stress fields and fold max|Vx|, max|Vy| into vmax (north-star item c).
 //
-// Arithmetic: divisions by dX, dY, 3 and rho are multiplications by reciprocals
-// computed once on the host, and the yield test compares J2^2 with coh^2 so that the
-// square root and the division by J2 run only in yielding cells.  Results differ from
-// the reference's division/sqrt forms by rounding only (parity tests: 1e-9).
+// Arithmetic: displacements and all arithmetic are FP64; velocities are stored as TV
+// (double on the plain path, float on the mixed path: velocities only scale the next
+// displacement increment, so their FP32 rounding is relative to a quantity that goes
+// to zero and leaves no floor on the convergence test).  Divisions by dX, dY, 3 and
+// rho are multiplications by host-computed reciprocals, and the yield test compares
+// J2^2 with coh^2 so that the square root and the division by J2 run only in yielding
+// cells.  Results differ from the reference's division/sqrt forms by rounding only.
 #pragma once
 
 #include "ep2d_types.hpp"
@@ -46,23 +50,24 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int TX, int TY, bool PLASTIC, bool RECORD>
-__global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
+template <int TX, int TY, bool PLASTIC, bool RECORD, typename TV>
+__device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const int src, const int bx, const int by,
+                                          TileSmem<TX, TY>& s) {
   static_assert(TX == 32 && TY % 8 == 0, "the thread mapping assumes 32 x 8 threads and TX == 32");
   using S = TileSmem<TX, TY>;
   constexpr int UW = S::UW, UH = S::UH, SW = S::SW, SH = S::SH, FW = S::FW, FH = S::FH;
   constexpr int RY = TY / 8;  // owned rows per thread
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S& s = *reinterpret_cast<S*>(smem_raw);
 
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i0 = bx * TX, j0 = by * TY;
   const int nx = g.nx, ny = g.ny;
   const size_t pitch = (size_t)g.pitch;
   const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
   const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
   double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
   double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
+  TV* __restrict__ fvx = static_cast<TV*>(f.vx);
+  TV* __restrict__ fvy = static_cast<TV*>(f.vy);
 
   // owned velocities, fetched first
   double vxr[RY], vyr[RY];
@@ -70,8 +75,8 @@ __global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
   for (int r = 0; r < RY; r++) {
     const int i = i0 + tx, j = j0 + ty + 8 * r;
     const bool ok = (i < nx && j < ny);
-    vxr[r] = ok ? f.vx[j * pitch + i] : 0.0;
-    vyr[r] = ok ? f.vy[j * pitch + i] : 0.0;
+    vxr[r] = ok ? (double)fvx[j * pitch + i] : 0.0;
+    vyr[r] = ok ? (double)fvy[j * pitch + i] : 0.0;
   }
 
   // ---- A: stage Ux (i in [i0-1, i0+TX+1], j in [j0-2, j0+TY]), Uy (i in [i0-2, i0+TX],
@@ -210,25 +215,29 @@ __global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
     if (i > 0 && j > 0 && j < ny - 1) {
       vx = vx * cX + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj + 1][li] + s.xx[lj + 1][li + 1] - s.xx[lj + 1][li]) * rdX +
                             (s.xy[lj + 2][li + 1] - s.xy[lj + 1][li + 1]) * rdY);
-      f.vx[q] = vx;
+      const TV vs = (TV)vx;
+      fvx[q] = vs;
+      vx = (double)vs;  // the displacement moves by the stored velocity
     }
     uxo[q] = s.ux[lj + 2][li + 1] + vx * dT;
     double vy = vyr[r];
     if (i > 0 && i < nx - 1 && j > 0) {
       vy = vy * cY + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj][li + 1] + s.yy[lj + 1][li + 1] - s.yy[lj][li + 1]) * rdY +
                             (s.xy[lj + 1][li + 2] - s.xy[lj + 1][li + 1]) * rdX);
-      f.vy[q] = vy;
+      const TV vs = (TV)vy;
+      fvy[q] = vs;
+      vy = (double)vs;
     }
     uyo[q] = s.uy[lj + 1][li + 2] + vy * dT;
     if (i == nx - 1) {  // face column i = nx of Ux/Vx: never updated by the reference
       const size_t q2 = j * pitch + nx;
       uxo[q2] = s.ux[lj + 2][li + 2];
-      if (RECORD) vmx = fmax(vmx, fabs(f.vx[q2]));
+      if (RECORD) vmx = fmax(vmx, fabs((double)fvx[q2]));
     }
     if (j == ny - 1) {  // face row j = ny of Uy/Vy
       const size_t q3 = (size_t)ny * pitch + i;
       uyo[q3] = s.uy[lj + 2][li + 2];
-      if (RECORD) vmy = fmax(vmy, fabs(f.vy[q3]));
+      if (RECORD) vmy = fmax(vmy, fabs((double)fvy[q3]));
     }
     if (RECORD) {
       vmx = fmax(vmx, fabs(vx));
@@ -248,6 +257,34 @@ __global__ void __launch_bounds__(256) k_iter_f64(Geo g, F64Fields f, int src) {
       atomic_max_nonneg(&f.vmax[0], vmx);
       atomic_max_nonneg(&f.vmax[1], vmy);
     }
+  }
+}
+
+// One RVE: one CTA per tile.
+template <int TX, int TY, bool PLASTIC, bool RECORD, typename TV>
+__global__ void __launch_bounds__(256) k_iter(Geo g, Fields f, int src) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  iter_tile<TX, TY, PLASTIC, RECORD, TV>(g, f, src, blockIdx.x, blockIdx.y,
+                                         *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw));
+}
+
+// Many RVEs: a persistent grid walks the device-side tile list {rve, bx | by << 16}.
+// The list and its length live in device memory, so a captured graph of these
+// launches stays valid while RVEs join and retire; `parity` is the launch's position
+// in the graph (mod 2), flipping every RVE's ping-pong buffers in lockstep.
+template <int TX, int TY, bool RECORD, typename TV>
+__global__ void __launch_bounds__(256) k_iter_batch(const BatchEntry* __restrict__ ents, const int2* __restrict__ tiles,
+                                                    const int* __restrict__ ntiles, int parity) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileSmem<TX, TY>& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
+  const int n = *ntiles;
+  for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    const int2 tc = tiles[t];
+    const BatchEntry& e = ents[tc.x];
+    const int src = e.src0 ^ parity;
+    if (e.plastic) iter_tile<TX, TY, true, RECORD, TV>(e.g, e.f, src, tc.y & 0xffff, tc.y >> 16, s);
+    else iter_tile<TX, TY, false, RECORD, TV>(e.g, e.f, src, tc.y & 0xffff, tc.y >> 16, s);
+    __syncthreads();  // shared memory is reused by the next tile
   }
 }
 

@@ -1,4 +1,5 @@
-// ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh.
+// ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh and
+// ep2d_iter_f64.cuh.
 #include "ep2d_device.cuh"
 #include "ep2d_iter_f64.cuh"
 
@@ -7,20 +8,114 @@ namespace ep2d {
 namespace {
 constexpr int kIterThreadsX = 32, kIterThreadsY = 8;
 
-template <bool PLASTIC, bool RECORD>
-cudaError_t set_iter_attr() {
-  return cudaFuncSetAttribute(k_iter_f64<TILE_X, TILE_Y, PLASTIC, RECORD>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(TileSmem<TILE_X, TILE_Y>));
+template <int TY>
+constexpr size_t smem_bytes() {
+  return sizeof(TileSmem<TILE_X, TY>);
+}
+
+template <int TY, bool PLASTIC, bool RECORD, typename TV>
+cudaError_t set_one_attr() {
+  return cudaFuncSetAttribute(k_iter<TILE_X, TY, PLASTIC, RECORD, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes<TY>());
+}
+
+template <int TY, bool RECORD, typename TV>
+cudaError_t set_batch_attr() {
+  return cudaFuncSetAttribute(k_iter_batch<TILE_X, TY, RECORD, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes<TY>());
+}
+
+template <int TY, typename TV>
+cudaError_t set_attrs_ty() {
+  cudaError_t e;
+  if ((e = set_one_attr<TY, false, false, TV>()) != cudaSuccess) return e;
+  if ((e = set_one_attr<TY, false, true, TV>()) != cudaSuccess) return e;
+  if ((e = set_one_attr<TY, true, false, TV>()) != cudaSuccess) return e;
+  if ((e = set_one_attr<TY, true, true, TV>()) != cudaSuccess) return e;
+  if ((e = set_batch_attr<TY, false, TV>()) != cudaSuccess) return e;
+  return set_batch_attr<TY, true, TV>();
+}
+
+template <int TY, typename TV>
+cudaError_t launch_iter_ty(const Geo& g, const Fields& f, int src, bool plastic, bool record, cudaStream_t stream) {
+  const dim3 block(kIterThreadsX, kIterThreadsY);
+  const dim3 grid((g.nx + TILE_X - 1) / TILE_X, (g.ny + TY - 1) / TY);
+  const size_t sm = smem_bytes<TY>();
+  if (plastic) {
+    if (record) k_iter<TILE_X, TY, true, true, TV><<<grid, block, sm, stream>>>(g, f, src);
+    else k_iter<TILE_X, TY, true, false, TV><<<grid, block, sm, stream>>>(g, f, src);
+  } else {
+    if (record) k_iter<TILE_X, TY, false, true, TV><<<grid, block, sm, stream>>>(g, f, src);
+    else k_iter<TILE_X, TY, false, false, TV><<<grid, block, sm, stream>>>(g, f, src);
+  }
+  return cudaGetLastError();
+}
+
+template <int TY, typename TV>
+cudaError_t launch_batch_ty(const BatchEntry* ents, const int2* tiles, const int* ntiles, int parity, bool record,
+                            int blocks, cudaStream_t stream) {
+  const dim3 block(kIterThreadsX, kIterThreadsY);
+  const size_t sm = smem_bytes<TY>();
+  if (record) k_iter_batch<TILE_X, TY, true, TV><<<blocks, block, sm, stream>>>(ents, tiles, ntiles, parity);
+  else k_iter_batch<TILE_X, TY, false, TV><<<blocks, block, sm, stream>>>(ents, tiles, ntiles, parity);
+  return cudaGetLastError();
+}
+
+template <int TY, typename TV>
+int occupancy_ty(bool record) {
+  int n = 0;
+  const cudaError_t e =
+      record ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_batch<TILE_X, TY, true, TV>, 256,
+                                                             smem_bytes<TY>())
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_batch<TILE_X, TY, false, TV>, 256,
+                                                             smem_bytes<TY>());
+  return e == cudaSuccess && n > 0 ? n : 1;
 }
 }  // namespace
 
 cudaError_t prepare_kernels() {
   cudaError_t e;
-  if ((e = set_iter_attr<false, false>()) != cudaSuccess) return e;
-  if ((e = set_iter_attr<false, true>()) != cudaSuccess) return e;
-  if ((e = set_iter_attr<true, false>()) != cudaSuccess) return e;
-  return set_iter_attr<true, true>();
+  if ((e = set_attrs_ty<8, double>()) != cudaSuccess) return e;
+  if ((e = set_attrs_ty<16, double>()) != cudaSuccess) return e;
+  if ((e = set_attrs_ty<32, double>()) != cudaSuccess) return e;
+  if ((e = set_attrs_ty<8, float>()) != cudaSuccess) return e;
+  if ((e = set_attrs_ty<16, float>()) != cudaSuccess) return e;
+  return set_attrs_ty<32, float>();
+}
+
+cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed, int tile_y,
+                        cudaStream_t stream) {
+  if (mixed) {
+    if (tile_y == 8) return launch_iter_ty<8, float>(g, f, src, plastic, record, stream);
+    if (tile_y == 32) return launch_iter_ty<32, float>(g, f, src, plastic, record, stream);
+    return launch_iter_ty<16, float>(g, f, src, plastic, record, stream);
+  }
+  if (tile_y == 8) return launch_iter_ty<8, double>(g, f, src, plastic, record, stream);
+  if (tile_y == 32) return launch_iter_ty<32, double>(g, f, src, plastic, record, stream);
+  return launch_iter_ty<16, double>(g, f, src, plastic, record, stream);
+}
+
+cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* tiles, const int* ntiles, int parity, bool record,
+                              bool mixed, int tile_y, int blocks, cudaStream_t stream) {
+  if (mixed) {
+    if (tile_y == 8) return launch_batch_ty<8, float>(ents, tiles, ntiles, parity, record, blocks, stream);
+    if (tile_y == 32) return launch_batch_ty<32, float>(ents, tiles, ntiles, parity, record, blocks, stream);
+    return launch_batch_ty<16, float>(ents, tiles, ntiles, parity, record, blocks, stream);
+  }
+  if (tile_y == 8) return launch_batch_ty<8, double>(ents, tiles, ntiles, parity, record, blocks, stream);
+  if (tile_y == 32) return launch_batch_ty<32, double>(ents, tiles, ntiles, parity, record, blocks, stream);
+  return launch_batch_ty<16, double>(ents, tiles, ntiles, parity, record, blocks, stream);
+}
+
+int iter_blocks_per_sm(bool record, bool mixed, int tile_y) {
+  if (mixed) {
+    if (tile_y == 8) return occupancy_ty<8, float>(record);
+    if (tile_y == 32) return occupancy_ty<32, float>(record);
+    return occupancy_ty<16, float>(record);
+  }
+  if (tile_y == 8) return occupancy_ty<8, double>(record);
+  if (tile_y == 32) return occupancy_ty<32, double>(record);
+  return occupancy_ty<16, double>(record);
 }
 
 cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream) {
@@ -30,27 +125,12 @@ cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_preload(const Geo& g, const F64Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
+cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
                            int zero_first, cudaStream_t stream) {
   const dim3 block(32, 8);
   const dim3 grid((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8);
   k_preload<<<grid, block, 0, stream>>>(g, f.ux[0], f.ux[1], f.uy[0], f.uy[1], src, dUxdx, dUydy, dUxdy,
                                         zero_first);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_iter_f64(const Geo& g, const F64Fields& f, int src, bool plastic, bool record,
-                            cudaStream_t stream) {
-  const dim3 block(kIterThreadsX, kIterThreadsY);
-  const dim3 grid((g.nx + TILE_X - 1) / TILE_X, (g.ny + TILE_Y - 1) / TILE_Y);
-  const size_t sm = sizeof(TileSmem<TILE_X, TILE_Y>);
-  if (plastic) {
-    if (record) k_iter_f64<TILE_X, TILE_Y, true, true><<<grid, block, sm, stream>>>(g, f, src);
-    else k_iter_f64<TILE_X, TILE_Y, true, false><<<grid, block, sm, stream>>>(g, f, src);
-  } else {
-    if (record) k_iter_f64<TILE_X, TILE_Y, false, true><<<grid, block, sm, stream>>>(g, f, src);
-    else k_iter_f64<TILE_X, TILE_Y, false, false><<<grid, block, sm, stream>>>(g, f, src);
-  }
   return cudaGetLastError();
 }
 
@@ -64,34 +144,35 @@ int avg_blocks(const Geo& g) {
 
 size_t avg_partials_len(const Geo& g) { return (size_t)avg_blocks(g) * NAVG; }
 
-cudaError_t launch_average(const Geo& g, const F64Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,
+cudaError_t launch_average(const Geo& g, const Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,
                            double* partials, double* sums, cudaStream_t stream) {
   const int nb = avg_blocks(g);
-  k_average<<<nb, 256, 0, stream>>>(g, f.p, f.txx, f.tyy, f.txy, src ? f.ux[1] : f.ux[0], src ? f.uy[1] : f.uy[0], nu0, perOffsetX,
-                                    perOffsetY, kAvgRowsPerBlock, partials);
+  k_average<<<nb, 256, 0, stream>>>(g, f.p, f.txx, f.tyy, f.txy, src ? f.ux[1] : f.ux[0], src ? f.uy[1] : f.uy[0],
+                                    nu0, perOffsetX, perOffsetY, kAvgRowsPerBlock, partials);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sum_partials<<<1, 32, 0, stream>>>(partials, nb, NAVG, sums);
   return cudaGetLastError();
 }
 
-cudaError_t launch_boundary(const Geo& g, const F64Fields& f, double* sums, cudaStream_t stream) {
+cudaError_t launch_boundary(const Geo& g, const Fields& f, double* sums, cudaStream_t stream) {
   k_boundary<<<1, 256, 0, stream>>>(g, f.p, f.txx, f.tyy, sums);
   return cudaGetLastError();
 }
 
-cudaError_t launch_gather(const Geo& g, const F64Fields& f, int src, const unsigned long long* idx, int n,
+cudaError_t launch_gather(const Geo& g, const Fields& f, int src, const unsigned long long* idx, int n,
                           double* out, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   k_gather<<<(n + 127) / 128, 128, 0, stream>>>(g, src ? f.ux[1] : f.ux[0], src ? f.uy[1] : f.uy[0], idx, n, out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_static_fields(const Geo& g, const F64Fields& f, int src, double* unu, double* j1, double* j2,
+cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double* unu, double* j1, double* j2,
                                  cudaStream_t stream) {
   const dim3 block(32, 8);
   const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
-  k_static_fields<<<grid, block, 0, stream>>>(g, src ? f.ux[1] : f.ux[0], src ? f.uy[1] : f.uy[0], f.p, f.txx, f.tyy, f.txy, unu, j1, j2);
+  k_static_fields<<<grid, block, 0, stream>>>(g, src ? f.ux[1] : f.ux[0], src ? f.uy[1] : f.uy[0], f.p, f.txx, f.tyy,
+                                              f.txy, unu, j1, j2);
   return cudaGetLastError();
 }
 

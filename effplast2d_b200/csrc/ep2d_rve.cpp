@@ -277,6 +277,8 @@ size_t n_samples(const ep2d_params& p) {
 
 std::mutex g_prep_mu;
 std::set<int> g_prepared;
+}  // namespace
+
 int prepare_device(int dev) {
   std::lock_guard<std::mutex> lk(g_prep_mu);
   if (g_prepared.count(dev)) return EP2D_OK;
@@ -285,7 +287,6 @@ int prepare_device(int dev) {
   g_prepared.insert(dev);
   return EP2D_OK;
 }
-}  // namespace
 
 size_t Rve::footprint(const ep2d_params& p) {
   const size_t fe = field_elems(p);
@@ -325,7 +326,6 @@ void Rve::release() {
 int Rve::create(const ep2d_params& p, cudaStream_t s) {
   int rc = validate_params(p);
   if (rc) return rc;
-  if (p.precision != EP2D_FP64) return fail(EP2D_ERR_ARG, "this RVE object runs the FP64 path only");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EP2D_ERR_NODEV, "no CUDA device");
   if (p.device < 0 || p.device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");
@@ -442,7 +442,7 @@ int Rve::reset() {
 }
 
 int Rve::launch_one(bool record) {
-  EP2D_CK(launch_iter_f64(g, f, cur, prm.nl > 1, record, stream));
+  EP2D_CK(launch_iter(g, f, cur, prm.nl > 1, record, mixed(), tile_y, stream));
   cur ^= 1;
   return EP2D_OK;
 }
@@ -454,7 +454,7 @@ int Rve::capture(int parity) {
   cur = parity;
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < kGraphLen && le == cudaSuccess; k++) {
-    le = launch_iter_f64(g, f, cur, prm.nl > 1, false, stream);
+    le = launch_iter(g, f, cur, prm.nl > 1, false, mixed(), tile_y, stream);
     cur ^= 1;
   }
   cur = saved;
@@ -563,12 +563,10 @@ int Rve::finish_time_step(int step, int it) {
   return EP2D_OK;
 }
 
-int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) {
+int Rve::begin_step(int step, int n_time_steps) {
   if (step < 0 || step >= prm.nl) return fail(EP2D_ERR_ARG, "step must be in [0, nl)");
   if (n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
-  if (!lt) return fail(EP2D_ERR_ARG, "load_type is null");
   if (step > 0 && !have_step0) return fail(EP2D_ERR_STATE, "increment step before the preload (step 0)");
-  DeviceScope ds(device);
   nts[step] = n_time_steps;
   rec[step].assign(n_time_steps, ep2d_step_record{});
   checks[step].assign(n_time_steps, std::vector<double>{});
@@ -576,6 +574,58 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
     ces[0] = ces[1] = ces[2] = 0.0;
     have_step0 = true;
   }
+  return EP2D_OK;
+}
+
+void Rve::begin_chain(const double lt[3]) {
+  std::memcpy(load_type_, lt, sizeof(load_type_));
+  an = an_per = num = num_per = ep2d_moduli{0.0, 0.0, 0.0};
+}
+
+// ComputeEffModuli's three load steps (EffPlast2D.cu:188-205): the preload, then the
+// spherical and deviatoric increments of incPercent = 0.005 (EffPlast2D.h:105)
+void Rve::step_load(int step, double init, const double lt[3], int nts, double* lsv, double lt_out[3], int* nts_out) {
+  const double incPercent = 0.005;
+  const double sph[3] = {0.5 * (lt[0] + lt[1]), 0.5 * (lt[0] + lt[1]), 0.0};
+  const double dev[3] = {lt[0] - sph[0], lt[1] - sph[1], lt[2]};
+  if (step == 0) {
+    *lsv = init;
+    std::memcpy(lt_out, lt, 3 * sizeof(double));
+    *nts_out = nts;
+  } else {
+    *lsv = init * incPercent;
+    std::memcpy(lt_out, step == 1 ? sph : dev, 3 * sizeof(double));
+    *nts_out = 1;
+  }
+}
+
+void Rve::finish_chain(int n_time_steps, ep2d_result* out) {
+  const ep2d_step_record& r0 = rec[0][n_time_steps - 1];
+  final_moduli(prm.nl, r0, prm.nl > 1 ? &rec[1][0] : nullptr, prm.nl == 3 ? &rec[2][0] : nullptr, &num, &num_per);
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->an = an;
+  out->an_per = an_per;
+  out->num = num;
+  out->num_per = num_per;
+  out->nl = prm.nl;
+  out->n_time_steps = n_time_steps;
+  int allc = 1;
+  int64_t tot = 0;
+  for (int a = 0; a < prm.nl; a++)
+    for (int t = 0; t < nts[a]; t++) {
+      tot += rec[a][t].iterations;
+      allc &= rec[a][t].converged;
+    }
+  out->total_iterations = tot;
+  out->all_converged = allc;
+}
+
+int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) {
+  if (!lt) return fail(EP2D_ERR_ARG, "load_type is null");
+  DeviceScope ds(device);
+  int rc0 = begin_step(step, n_time_steps);
+  if (rc0) return rc0;
   const int64_t ce = prm.check_every;
   for (int it = 0; it < n_time_steps; it++) {
     int rc = begin_time_step(step, it, lsv, lt, n_time_steps);
@@ -626,41 +676,15 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
 int Rve::compute_eff_moduli(double init, const double lt[3], int n_time_steps, ep2d_result* out) {
   if (!lt) return fail(EP2D_ERR_ARG, "load_type is null");
   if (n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
-  const double incPercent = 0.005;  // EffPlast2D.h:105
-  std::memcpy(load_type_, lt, sizeof(load_type_));
-  const double sph[3] = {0.5 * (lt[0] + lt[1]), 0.5 * (lt[0] + lt[1]), 0.0};
-  const double dev[3] = {lt[0] - sph[0], lt[1] - sph[1], lt[2]};
-  an = an_per = num = num_per = ep2d_moduli{0.0, 0.0, 0.0};
-  int rc = solve_step(0, init, lt, n_time_steps);
-  if (rc) return rc;
-  if (prm.nl > 1) {
-    rc = solve_step(1, init * incPercent, sph, 1);
+  begin_chain(lt);
+  for (int step = 0; step < prm.nl; step++) {
+    double lsv, lts[3];
+    int ns;
+    step_load(step, init, lt, n_time_steps, &lsv, lts, &ns);
+    const int rc = solve_step(step, lsv, lts, ns);
     if (rc) return rc;
   }
-  if (prm.nl == 3) {
-    rc = solve_step(2, init * incPercent, dev, 1);
-    if (rc) return rc;
-  }
-  const ep2d_step_record& r0 = rec[0][n_time_steps - 1];
-  final_moduli(prm.nl, r0, prm.nl > 1 ? &rec[1][0] : nullptr, prm.nl == 3 ? &rec[2][0] : nullptr, &num, &num_per);
-  if (out) {
-    std::memset(out, 0, sizeof(*out));
-    out->an = an;
-    out->an_per = an_per;
-    out->num = num;
-    out->num_per = num_per;
-    out->nl = prm.nl;
-    out->n_time_steps = n_time_steps;
-    int allc = 1;
-    int64_t tot = 0;
-    for (int a = 0; a < prm.nl; a++)
-      for (int t = 0; t < nts[a]; t++) {
-        tot += rec[a][t].iterations;
-        allc &= rec[a][t].converged;
-      }
-    out->total_iterations = tot;
-    out->all_converged = allc;
-  }
+  finish_chain(n_time_steps, out);
   return EP2D_OK;
 }
 
@@ -702,8 +726,17 @@ int Rve::get_field(int field, double* host) const {
     case EP2D_FIELD_J2XY: src = f.j2xy; break;
     case EP2D_FIELD_UX: src = f.ux[cur]; break;
     case EP2D_FIELD_UY: src = f.uy[cur]; break;
-    case EP2D_FIELD_VX: src = f.vx; break;
-    case EP2D_FIELD_VY: src = f.vy; break;
+    case EP2D_FIELD_VX: src = static_cast<const double*>(f.vx); break;
+    case EP2D_FIELD_VY: src = static_cast<const double*>(f.vy); break;
+  }
+  if (mixed() && (field == EP2D_FIELD_VX || field == EP2D_FIELD_VY)) {  // float storage
+    std::vector<float> tmp((size_t)w * h);
+    EP2D_CK(cudaMemcpy2DAsync(tmp.data(), (size_t)w * sizeof(float), field == EP2D_FIELD_VX ? f.vx : f.vy,
+                              (size_t)g.pitch * sizeof(float), (size_t)w * sizeof(float), h, cudaMemcpyDeviceToHost,
+                              stream));
+    EP2D_CK(cudaStreamSynchronize(stream));
+    for (size_t k = 0; k < tmp.size(); k++) host[k] = tmp[k];
+    return EP2D_OK;
   }
   EP2D_CK(cudaMemcpy2DAsync(host, (size_t)w * sizeof(double), src, pb, (size_t)w * sizeof(double), h,
                             cudaMemcpyDeviceToHost, stream));
@@ -730,8 +763,16 @@ int Rve::set_field(int field, const double* host) {
     case EP2D_FIELD_J2XY: dst[0] = f.j2xy; break;
     case EP2D_FIELD_UX: dst[0] = f.ux[0]; dst[1] = f.ux[1]; break;
     case EP2D_FIELD_UY: dst[0] = f.uy[0]; dst[1] = f.uy[1]; break;
-    case EP2D_FIELD_VX: dst[0] = f.vx; break;
-    case EP2D_FIELD_VY: dst[0] = f.vy; break;
+    case EP2D_FIELD_VX: dst[0] = static_cast<double*>(f.vx); break;
+    case EP2D_FIELD_VY: dst[0] = static_cast<double*>(f.vy); break;
+  }
+  if (mixed() && (field == EP2D_FIELD_VX || field == EP2D_FIELD_VY)) {  // float storage
+    std::vector<float> tmp((size_t)w * h);
+    for (size_t k = 0; k < tmp.size(); k++) tmp[k] = (float)host[k];
+    EP2D_CK(cudaMemcpy2DAsync(field == EP2D_FIELD_VX ? f.vx : f.vy, (size_t)g.pitch * sizeof(float), tmp.data(),
+                              (size_t)w * sizeof(float), (size_t)w * sizeof(float), h, cudaMemcpyHostToDevice, stream));
+    EP2D_CK(cudaStreamSynchronize(stream));
+    return EP2D_OK;
   }
   for (double* dp : dst)
     if (dp)

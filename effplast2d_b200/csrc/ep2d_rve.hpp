@@ -56,6 +56,9 @@ int validate_params(const ep2d_params& p);
 // Device row pitch (elements) for an nx-wide grid.
 int row_pitch(int nx);
 
+// Per-device kernel attributes, once per device (the device must be current).
+int prepare_device(int dev);
+
 class Rve {
  public:
   Rve() = default;
@@ -78,6 +81,12 @@ class Rve {
                          ep2d_result* out);
 
   // building blocks (used by solve_step, by the batch solver and by the tests)
+  void begin_chain(const double load_type[3]);  // ComputeEffModuli's prologue
+  // load value, load type and time steps of load step `step` of the chain
+  static void step_load(int step, double init, const double lt[3], int nts, double* lsv, double lt_out[3],
+                        int* nts_out);
+  int begin_step(int step, int n_time_steps);   // ComputeEffParams' prologue
+  void finish_chain(int n_time_steps, ep2d_result* out);  // calc* and the result
   int begin_time_step(int step, int it, double load_step_value, const double load_type[3], int n_time_steps);
   int iterate(int64_t n, bool record_last);  // n iterations; the last one records stresses
   int launch_one(bool record);                // one iteration kernel (no stats)
@@ -97,7 +106,9 @@ class Rve {
   ep2d_params prm{};
   Derived d{};
   Geo g{};
-  F64Fields f{};
+  Fields f{};
+  int tile_y = TILE_Y;  // tile height of the iteration kernel
+  bool mixed() const { return prm.precision == EP2D_MIXED; }
   int cur = 0;
   int device = 0;
   cudaStream_t stream = nullptr;

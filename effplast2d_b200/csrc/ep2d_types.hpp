@@ -21,39 +21,56 @@ struct Geo {
   double rdX, rdY, coh2, cX, cY, dtr;
 };
 
-// Device pointers of one RVE on the FP64 path.
-struct F64Fields {
+// Device pointers of one RVE.  Velocities are stored as double on the FP64 path and as
+// float on the mixed path (the launch selects the type); everything else is double.
+struct Fields {
   double* ux[2];
   double* uy[2];
-  double* vx;
-  double* vy;
+  void* vx;
+  void* vy;
   double *p, *txx, *tyy, *txy, *txyav, *j2, *j2xy;  // last recorded stress state
   const uint8_t* mask;
   unsigned long long* vmax;  // [2]: bit patterns of max|Vx|, max|Vy| (non-negative)
 };
 
-// Tile of the fused iteration kernel.
+// One RVE of a batched launch.
+struct BatchEntry {
+  Geo g;
+  Fields f;
+  int src0;     // ping-pong buffer holding U at the start of the current graph
+  int plastic;  // NL > 1
+};
+
+// Tile of the fused iteration kernel: 32 columns x TILE_Y rows; the tile height is a
+// launch-time choice among TILE_Y_CHOICES (the batch autotuner picks it).
 constexpr int TILE_X = 32;
 constexpr int TILE_Y = 16;
+constexpr int TILE_Y_CHOICES[3] = {8, 16, 32};
 
 // Number of sums produced by the averaging and boundary reductions.
 constexpr int NAVG = 11;
 
 // Launch wrappers (ep2d_kernels.cu).  All are asynchronous on `stream`.
-cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream);
-cudaError_t launch_preload(const Geo& g, const F64Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
-                           int zero_first, cudaStream_t stream);
-cudaError_t launch_iter_f64(const Geo& g, const F64Fields& f, int src, bool plastic, bool record,
-                            cudaStream_t stream);
 cudaError_t prepare_kernels();  // per-device function attributes
+cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream);
+cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
+                           int zero_first, cudaStream_t stream);
+// one iteration of one RVE; mixed: velocities stored as float
+cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed, int tile_y,
+                        cudaStream_t stream);
+// one iteration of every RVE in the tile list (persistent grid of `blocks` CTAs)
+cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* tiles, const int* ntiles, int parity, bool record,
+                              bool mixed, int tile_y, int blocks, cudaStream_t stream);
+// CTAs of one tile height resident per SM (occupancy of the batched kernel)
+int iter_blocks_per_sm(bool record, bool mixed, int tile_y);
 // averaging: writes NAVG sums to `sums` (device); `partials` holds avg_partials_len(g) doubles
 size_t avg_partials_len(const Geo& g);
-cudaError_t launch_average(const Geo& g, const F64Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,
+cudaError_t launch_average(const Geo& g, const Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,
                            double* partials, double* sums, cudaStream_t stream);
-cudaError_t launch_boundary(const Geo& g, const F64Fields& f, double* sums, cudaStream_t stream);
-cudaError_t launch_gather(const Geo& g, const F64Fields& f, int src, const unsigned long long* idx, int n,
+cudaError_t launch_boundary(const Geo& g, const Fields& f, double* sums, cudaStream_t stream);
+cudaError_t launch_gather(const Geo& g, const Fields& f, int src, const unsigned long long* idx, int n,
                           double* out, cudaStream_t stream);
-cudaError_t launch_static_fields(const Geo& g, const F64Fields& f, int src, double* unu, double* j1, double* j2,
+cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double* unu, double* j1, double* j2,
                                  cudaStream_t stream);
 
 // Scalars of the analytic static solution (SaveAnStatic2D, EffPlast2D.cu:1062-1078).

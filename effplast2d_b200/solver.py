@@ -22,6 +22,8 @@ EXPORTS = (
     "ep2d_field_dims", "ep2d_create", "ep2d_destroy", "ep2d_reset", "ep2d_iterate", "ep2d_get_field",
     "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
+    "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
+    "ep2d_server_stats", "ep2d_server_destroy",
 )
 
 
@@ -60,6 +62,15 @@ def lib():
         L.ep2d_analytic_fields.argtypes = [vp, d, d] + [P(d)] * 7
         L.ep2d_abi_sizes.argtypes = [P(i64), i32]
         L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64), P(i64)]
+        L.ep2d_batch_solve.argtypes = [P(_abi.BatchConfig), P(_abi.RveSpec), i32, P(_abi.Result),
+                                       P(_abi.BatchStats)]
+        L.ep2d_rve_footprint.argtypes = [P(_abi.RveSpec), i32]
+        L.ep2d_rve_footprint.restype = i64
+        L.ep2d_server_create.argtypes = [P(_abi.BatchConfig), i64, i32, P(vp)]
+        L.ep2d_server_submit.argtypes = [vp, P(_abi.RveSpec), P(ctypes.c_uint64)]
+        L.ep2d_server_wait.argtypes = [vp, ctypes.c_uint64, i32, P(i32), P(_abi.Result), P(d), P(d)]
+        L.ep2d_server_stats.argtypes = [vp, P(i64), P(i64), P(i64), P(i64), P(_abi.BatchStats)]
+        L.ep2d_server_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -99,10 +110,11 @@ def write_pa(path, pa):
 class Solver:
     """One RVE on the GPU (an ep2d_handle): the reference's EffPlast2D object."""
 
-    def __init__(self, nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000, device=0):
+    def __init__(self, nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000, device=0,
+                 precision=_abi.FP64):
         self.nx, self.ny = int(nx), int(ny)
         self.params = _abi.make_params(nx, ny, pa, nl=nl, niter=niter, eiter=eiter,
-                                       check_every=check_every, precision=_abi.FP64, device=device)
+                                       check_every=check_every, precision=precision, device=device)
         h = ctypes.c_void_p()
         _check(lib().ep2d_create(ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h

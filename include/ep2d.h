@@ -44,7 +44,8 @@ enum {
 /* arithmetic of the pseudo-transient stencil */
 enum {
   EP2D_FP64 = 0,         /* plain path: every field and every operation in FP64 */
-  EP2D_MIXED = 1         /* FP32 stencil bulk; FP64 residual, averages and moduli */
+  EP2D_MIXED = 1         /* velocities stored in FP32 (half their HBM traffic); displacements,
+                            stencil arithmetic, residual, averages and moduli in FP64 */
 };
 
 /* pa.dat layout (get_sigma_2D.m:32, read at EffPlast2D.cu:700-707, used at :1563-1573) */
@@ -127,6 +128,43 @@ typedef struct ep2d_result {
 
 typedef struct ep2d_handle ep2d_handle;
 
+/* ---- batches and serving (no counterpart in the reference, which solves one RVE per
+ * process; each RVE below is what one run of the reference's binary computes) ------- */
+
+/* One homogenisation request: the inputs of one reference run (pa.dat, NGRID, NL and
+ * the CLI's load arguments, main.cu:12-14). */
+typedef struct ep2d_rve_spec {
+  int32_t nx, ny;
+  double pa[EP2D_NPARS];
+  int32_t nl;
+  int32_t n_time_steps;
+  double init_load_value;
+  double load_type[3];
+} ep2d_rve_spec;
+
+/* Settings shared by every RVE of a batch. */
+typedef struct ep2d_batch_config {
+  int64_t niter;          /* NITER (a multiple of check_every) */
+  double eiter;           /* EITER */
+  int32_t check_every;    /* output_step */
+  int32_t precision;      /* EP2D_FP64 or EP2D_MIXED (FP32 velocity storage) */
+  int32_t device;
+  int32_t tile_y;         /* 8, 16 or 32 rows per tile; 0 = pick by timing the first launches */
+  int32_t graph_len;      /* iterations per captured CUDA graph (even; 0 = 64) */
+  int32_t reserved;
+} ep2d_batch_config;
+
+typedef struct ep2d_batch_stats {
+  double kernel_ms;       /* device time of the iteration launches (CUDA events) */
+  double wall_ms;
+  int64_t launches;       /* batched iteration launches */
+  int64_t all_launches;   /* every kernel launched, post-processing included */
+  int64_t cell_updates;   /* sum over RVEs of nx*ny per iteration */
+  int32_t tile_y;         /* tile height used */
+  int32_t blocks;         /* persistent grid size */
+  double tune_us[3];      /* measured us per launch for tile heights 8, 16, 32 (0 if untimed) */
+} ep2d_batch_stats;
+
 /* ---- library ---------------------------------------------------------------- */
 const char* ep2d_version(void);
 const char* ep2d_last_error(void);
@@ -202,8 +240,39 @@ int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, doubl
                          double* error_uabs, double* j1an, double* j2an, double* error_j1,
                          double* error_j2, double stats[6]);
 
-/* sizeof(ep2d_params), sizeof(ep2d_step_record), sizeof(ep2d_moduli), sizeof(ep2d_result)
- * into out[0..n); returns the number of structs (4).  Lets a binding check its layout. */
+/* ---- batch ---------------------------------------------------------------------- */
+/* Solve n RVEs together: every RVE runs ComputeEffModuli's chain (EffPlast2D.cu:179-229)
+ * with the reference's convergence test and checkpoint cadence; all active RVEs advance
+ * in lockstep through one persistent batched kernel per iteration, captured in a CUDA
+ * graph; finished RVEs retire at their checkpoint.  results[k] is what the reference
+ * binary would compute for specs[k].  Fails with EP2D_ERR_NOMEM if the RVEs do not fit
+ * on the device at once (the server admits them progressively instead). */
+int ep2d_batch_solve(const ep2d_batch_config* cfg, const ep2d_rve_spec* specs, int32_t n,
+                     ep2d_result* results, ep2d_batch_stats* stats);
+/* device bytes one RVE of this spec holds while it is being solved */
+int64_t ep2d_rve_footprint(const ep2d_rve_spec* spec, int32_t precision);
+
+/* ---- server (continuous batching) ------------------------------------------------- */
+typedef struct ep2d_server ep2d_server;
+/* A worker thread owns one batch engine on `cfg->device`.  Requests are admitted at
+ * checkpoint boundaries while the summed footprint of the active RVEs stays within
+ * mem_budget_bytes and their number within max_active; admitted RVEs stay resident
+ * until they converge. */
+int ep2d_server_create(const ep2d_batch_config* cfg, int64_t mem_budget_bytes, int32_t max_active,
+                       ep2d_server** out);
+int ep2d_server_submit(ep2d_server* s, const ep2d_rve_spec* spec, uint64_t* ticket_out);
+/* Wait up to timeout_ms (negative: forever) for the request to finish.  *done = 1 and
+ * *result / *latency_s (submit to completion, host clock) are filled when it has. */
+int ep2d_server_wait(ep2d_server* s, uint64_t ticket, int32_t timeout_ms, int32_t* done,
+                     ep2d_result* result, double* latency_s, double* queue_s);
+/* requests submitted, admitted, finished; bytes of device memory in use */
+int ep2d_server_stats(ep2d_server* s, int64_t* submitted, int64_t* admitted, int64_t* finished,
+                      int64_t* bytes_in_use, ep2d_batch_stats* engine);
+int ep2d_server_destroy(ep2d_server* s);
+
+/* sizeof() of ep2d_params, ep2d_step_record, ep2d_moduli, ep2d_result, ep2d_rve_spec,
+ * ep2d_batch_config and ep2d_batch_stats into out[0..n); returns the number of structs
+ * (7).  Lets a binding check its layout. */
 int ep2d_abi_sizes(int64_t* out, int32_t n);
 
 /* Counters of this handle since creation: device time of the iteration loops measured

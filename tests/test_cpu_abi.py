@@ -32,10 +32,11 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts_match():
-    out = (ctypes.c_int64 * 4)()
-    n = ep.lib().ep2d_abi_sizes(out, 4)
-    assert n == 4
-    sizes = [ctypes.sizeof(s) for s in (_abi.Params, _abi.StepRecord, _abi.Moduli, _abi.Result)]
+    out = (ctypes.c_int64 * 7)()
+    n = ep.lib().ep2d_abi_sizes(out, 7)
+    assert n == 7
+    sizes = [ctypes.sizeof(s) for s in (_abi.Params, _abi.StepRecord, _abi.Moduli, _abi.Result, _abi.RveSpec,
+                                        _abi.BatchConfig, _abi.BatchStats)]
     assert list(out) == sizes
 
 

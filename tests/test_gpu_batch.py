@@ -1,0 +1,114 @@
+"""Batched persistent solver and continuous-batching server.
+
+Each RVE of a batch must give what the single-RVE path gives for the same inputs (the
+batched kernel runs the same per-tile code; the tile height chosen by the autotuner
+does not change any cell's arithmetic), the mixed-precision batch must stay within the
+north-star bar of 1e-5 relative on K_phi, K_d and G, and the server must return the
+same result for a request alone and in a mix.
+"""
+import math
+
+import pytest
+
+import effplast2d_b200 as ep
+from effplast2d_b200 import batch as B
+
+pytestmark = pytest.mark.gpu
+
+NITER, CE = 6000, 500
+
+
+def mk(n, n_pores, phi, Y, nl, load, lt, nts):
+    pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=Y, porosity=phi, n_pores=n_pores)
+    return B.spec(n, pa, nl, nts, load, lt)
+
+
+SPECS = [
+    (64, 1, 0.005, 1.0, 1, -4e-5, (1.0, 1.0, 0.0), 1),
+    (96, 3, 0.02, 1e-5, 3, -6e-5, (1.0, 0.8, 0.3), 2),
+    (64, 2, 0.02, 1e-5, 2, -6e-5, (1.0, 1.0, 0.0), 2),
+    (128, 1, 0.01, 2e-5, 3, -5e-5, (0.9, 1.0, 0.2), 1),
+    (80, 2, 0.03, 1e-5, 2, -3e-5, (1.0, 1.0, 0.1), 1),
+    (100, 4, 0.02, 5e-6, 3, -7e-5, (1.0, 0.6, 0.4), 1),
+]
+
+
+def single(sp, precision=ep.FP64):
+    args = sp
+    n, npo, phi, Y, nl, load, lt, nts = args
+    pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=Y, porosity=phi, n_pores=npo)
+    s = ep.Solver(n, n, pa, nl=nl, niter=NITER, eiter=1e-9, check_every=CE)
+    return s.compute_eff_moduli(load, list(lt), nts)
+
+
+def same(a, b, rtol):
+    if a == b or (math.isnan(a) and math.isnan(b)):
+        return True
+    return abs(a - b) <= rtol * abs(b)
+
+
+def check_result(r, ref, rtol, nl):
+    assert r["total_iterations"] == ref["total_iterations"]
+    keys = ["kphi", "kd"] + (["g"] if nl == 3 else [])
+    for kind in ("num", "num_per", "an", "an_per"):
+        for k in keys:
+            assert same(r[kind][k], ref[kind][k], rtol), (kind, k, r[kind][k], ref[kind][k])
+
+
+@pytest.mark.parametrize("tile_y", [0, 8, 32])
+def test_batch_matches_single_fp64(tile_y):
+    specs = [mk(*s) for s in SPECS]
+    res, st = B.batch_solve(specs, niter=NITER, eiter=1e-9, check_every=CE, tile_y=tile_y)
+    assert st["launches"] > 0 and st["tile_y"] in (8, 16, 32)
+    if tile_y:
+        assert st["tile_y"] == tile_y
+    for sp, r in zip(SPECS, res):
+        check_result(r, single(sp), 1e-12, sp[4])
+
+
+def test_batch_mixed_precision_moduli_error():
+    # FP32 velocity storage: moduli within 1e-5 of the FP64 path (measured ~1e-10)
+    specs = [mk(*s) for s in SPECS]
+    res, _ = B.batch_solve(specs, niter=NITER, eiter=1e-9, check_every=CE, precision=ep.MIXED)
+    for sp, r in zip(SPECS, res):
+        ref = single(sp)
+        keys = ["kphi", "kd"] + (["g"] if sp[4] == 3 else [])
+        for k in keys:
+            a, b = r["num"][k], ref["num"][k]
+            if math.isfinite(b):
+                assert abs(a - b) <= 1e-5 * abs(b), (sp, k, a, b)
+
+
+def test_server_result_same_alone_and_in_mix():
+    target = mk(*SPECS[1])
+    others = [mk(*s) for s in SPECS]
+    with B.Server(mem_budget_bytes=1 << 34, niter=NITER, eiter=1e-9, check_every=CE) as srv:
+        t_alone = srv.submit(target)
+        alone, lat_alone, _ = srv.wait(t_alone)
+    with B.Server(mem_budget_bytes=1 << 34, niter=NITER, eiter=1e-9, check_every=CE) as srv:
+        tickets = [srv.submit(s) for s in others[:3]]
+        t_mix = srv.submit(target)
+        tickets += [srv.submit(s) for s in others[3:]]
+        mix, lat_mix, _ = srv.wait(t_mix)
+        for t in tickets:
+            assert srv.wait(t, timeout_ms=600000) is not None
+        st = srv.stats()
+    assert st["finished"] == len(others) + 1
+    check_result(mix, alone, 1e-12, SPECS[1][4])
+    assert lat_alone > 0 and lat_mix > 0
+
+
+def test_server_admission_by_memory_budget():
+    # a budget that fits about one RVE at a time: requests queue, all complete in order
+    specs = [mk(*s) for s in SPECS[:4]]
+    biggest = max(B.footprint(s) for s in specs)
+    with B.Server(mem_budget_bytes=biggest + 1, niter=NITER, eiter=1e-9, check_every=CE) as srv:
+        tickets = [srv.submit(s) for s in specs]
+        outs = [srv.wait(t, timeout_ms=600000) for t in tickets]
+        st = srv.stats()
+    assert all(o is not None for o in outs)
+    assert st["admitted"] == len(specs)
+    # queueing happened: later requests waited in the queue
+    assert max(o[2] for o in outs) > 0.0
+    for sp, o in zip(SPECS[:4], outs):
+        check_result(o[0], single(sp), 1e-12, sp[4])
