@@ -131,6 +131,22 @@ def dist_setup():
     return world, rank, local
 
 
+def shard(n_items, rank, world):
+    """RVE indices this rank solves: independent units, round-robin, no overlap."""
+    return list(range(rank, n_items, world))
+
+
+def reduce_over_ranks(values, op, device=None):
+    """max / sum of a list of floats over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.cpu()]
+
+
 def cpu_sample(w, seconds=12.0, threads=None):
     """The CPU restatement of the reference on `threads` host threads, iterating the
     workload's preloaded state: returns (cell updates per second, threads, description)."""
@@ -231,6 +247,9 @@ def run_ours(args, w):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # the job: world * steps independent RVE solves, round-robin over the ranks
+    mine = shard(world * args.steps, rank, world)
+    assert len(mine) == args.steps
     # value: resident handle, each step = reset (a fresh object) + full chain
     s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"], device=dev)
     res = None
@@ -278,20 +297,9 @@ def run_ours(args, w):
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
-    # max over ranks
-    t = torch.tensor([ms, e2e_ms, float(st1["all_launches"] - st0["all_launches"])], dtype=torch.float64,
-                     device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms, e2e_ms = float(mx[0]), float(mx[1])
-        launches = int(sm[2])
-    else:
-        launches = int(t[2])
+    # device time: max over ranks; kernel launches: summed over ranks
+    ms, e2e_ms = reduce_over_ranks([ms, e2e_ms], "max", device="cuda")
+    launches = int(reduce_over_ranks([float(st1["all_launches"] - st0["all_launches"])], "sum", device="cuda")[0])
 
     # roofline of the fused iteration kernel over the timed region
     it_launches = st1["launches"] - st0["launches"]
