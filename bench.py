@@ -378,17 +378,127 @@ def run_kernel_only(args, w):
     return 0
 
 
+def sample_requests(count, seed, sides=(256, 512, 768, 1024)):
+    """Seeded RVEs with the batched/served workload's distributions: grid side uniform in
+    `sides`, nPores uniform in 1..4, porosity U(0.005, 0.05), Y log-uniform in
+    [5e-6, 5e-5], preload magnitude U(2e-5, 8e-5) along a random unit load type with
+    |xy| <= 0.5 (compressive xx, yy), NL uniform in {2, 3}, one time step."""
+    import math
+
+    import numpy as np
+
+    from effplast2d_b200 import batch as B
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(sides))
+        npores = int(rng.integers(1, 5))
+        phi = float(rng.uniform(0.005, 0.05))
+        yld = float(math.exp(rng.uniform(math.log(5e-6), math.log(5e-5))))
+        mag = float(rng.uniform(2e-5, 8e-5))
+        th = float(rng.uniform(math.pi / 8, 3 * math.pi / 8))
+        lt = np.array([math.cos(th), math.sin(th), float(rng.uniform(-0.5, 0.5))])
+        lt /= np.linalg.norm(lt)
+        nl = int(rng.integers(2, 4))
+        pa = make_pa({"n": n, "g0": 0.5, "yield_stress": yld, "porosity": phi, "n_pores": npores})
+        out.append({"spec": B.spec(n, pa, nl, 1, -mag, tuple(lt)), "n": n, "nl": nl, "pa": pa, "load": -mag,
+                    "lt": list(lt)})
+    return out
+
+
+def run_batch(args):
+    """Batched mixed-precision solve of a seeded set of RVEs against the plain FP64
+    single-RVE path solving the same RVEs one at a time."""
+    import numpy as np
+    import torch
+
+    import effplast2d_b200 as ep
+    from effplast2d_b200 import batch as B
+
+    reqs = sample_requests(args.batch_size, args.seed)
+    niter = 2_000_000
+    t = time.perf_counter()
+    res_b, st = B.batch_solve([r["spec"] for r in reqs], niter=niter, eiter=1e-9, check_every=10_000,
+                              precision=ep.MIXED)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t
+    t = time.perf_counter()
+    res_s = []
+    for r in reqs:
+        s = ep.Solver(r["n"], r["n"], r["pa"], nl=r["nl"], niter=niter, eiter=1e-9, check_every=10_000)
+        res_s.append(s.compute_eff_moduli(r["load"], r["lt"], 1))
+        s.close()
+    t_single = time.perf_counter() - t
+    errs = {k: [] for k in ("kphi", "kd", "g")}
+    for rb, rs, r in zip(res_b, res_s, reqs):
+        for k in errs:
+            if k == "g" and r["nl"] < 3:
+                continue
+            a, b = rb["num"][k], rs["num"][k]
+            if np.isfinite(b) and b != 0:
+                errs[k].append(abs(a - b) / abs(b))
+    cells = sum(r["n"] ** 2 * rs["total_iterations"] for r, rs in zip(reqs, res_s))
+    print(json.dumps({
+        "workload": "batch", "rves": len(reqs), "seed": args.seed, "precision": "mixed (FP32 velocities)",
+        "batched_solves_per_s": len(reqs) / t_batch, "single_fp64_solves_per_s": len(reqs) / t_single,
+        "speedup": t_single / t_batch, "batched_cell_updates_per_s": cells / t_batch,
+        "max_rel_moduli_error": {k: (max(v) if v else None) for k, v in errs.items()},
+        "tile_y": st["tile_y"], "tune_us": st["tune_us"], "blocks": st["blocks"],
+        "sides": sorted({r["n"] for r in reqs})}))
+    return 0
+
+
+def run_serve(args):
+    """Poisson stream of requests into the continuous-batching server: p50/p99 latency
+    and solves/s, with the plain FP64 one-at-a-time path's solves/s beside them."""
+    import numpy as np
+
+    import effplast2d_b200 as ep
+    from effplast2d_b200 import batch as B
+
+    reqs = sample_requests(args.batch_size, args.seed, sides=(256, 512, 768, 1024, 2048))
+    rng = np.random.default_rng(args.seed + 1)
+    gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
+    niter = 2_000_000
+    with B.Server(mem_budget_bytes=int(180e9), niter=niter, eiter=1e-9, check_every=10_000,
+                  precision=ep.MIXED) as srv:
+        t0 = time.perf_counter()
+        tickets = []
+        for r, gap in zip(reqs, gaps):
+            time.sleep(gap)
+            tickets.append(srv.submit(r["spec"]))
+        outs = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    lat = np.array([o[1] for o in outs])
+    print(json.dumps({
+        "workload": "serve", "requests": len(reqs), "rate_per_s": args.rate, "seed": args.seed,
+        "precision": "mixed (FP32 velocities)", "solves_per_s": len(reqs) / wall,
+        "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+        "queue_p50_s": float(np.percentile([o[2] for o in outs], 50)),
+        "all_converged": all(o[0]["all_converged"] for o in outs), "engine": st["engine"]}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--batch-size", type=int, default=32, help="RVEs of the batch / serve workloads")
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--rate", type=float, default=2.0, help="request rate of the serve workload (1/s)")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
                     help="run N iterations of the workload's preload step and report the kernel timing")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     w = WORKLOADS[args.workload]
     if args.kernel_only:
         return run_kernel_only(args, w)
