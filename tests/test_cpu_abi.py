@@ -107,3 +107,19 @@ def test_invalid_params_rejected_before_device(bad):
     with pytest.raises(ep.EP2DError) as e:
         ep.Solver(nx, nx, pa, nl=nl)
     assert e.value.status == _abi.ERR_ARG
+
+
+def test_batch_and_server_argument_errors():
+    # configuration checks happen before any device call
+    from effplast2d_b200 import batch as B
+
+    pa = ep.make_pa(20.0, 20.0, 64, 64)
+    s = B.spec(64, pa, 2, 1, -6e-5, (1.0, 1.0, 0.0))
+    assert B.footprint(s) > 64 * 65 * 8 * 13
+    assert B.footprint(s, ep.MIXED) == B.footprint(s)  # same allocation, half of V unused
+    with pytest.raises(ep.EP2DError) as e:  # niter not a multiple of check_every
+        B.batch_solve([s], niter=1500, check_every=1000)
+    assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)
+    with pytest.raises(ep.EP2DError) as e:
+        B.batch_solve([s], niter=2000, check_every=1000, tile_y=12)
+    assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)
