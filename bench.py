@@ -417,7 +417,7 @@ def run_batch(args):
     from effplast2d_b200 import batch as B
 
     reqs = sample_requests(args.batch_size, args.seed)
-    niter = 2_000_000
+    niter = args.niter
     t = time.perf_counter()
     res_b, st = B.batch_solve([r["spec"] for r in reqs], niter=niter, eiter=1e-9, check_every=10_000,
                               precision=ep.MIXED)
@@ -460,7 +460,7 @@ def run_serve(args):
     reqs = sample_requests(args.batch_size, args.seed, sides=(256, 512, 768, 1024, 2048))
     rng = np.random.default_rng(args.seed + 1)
     gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
-    niter = 2_000_000
+    niter = args.niter
     with B.Server(mem_budget_bytes=int(180e9), niter=niter, eiter=1e-9, check_every=10_000,
                   precision=ep.MIXED) as srv:
         t0 = time.perf_counter()
@@ -486,6 +486,7 @@ def main():
     ap.add_argument("--batch-size", type=int, default=32, help="RVEs of the batch / serve workloads")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--rate", type=float, default=2.0, help="request rate of the serve workload (1/s)")
+    ap.add_argument("--niter", type=int, default=2_000_000, help="NITER of the batch / serve workloads")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
                     help="run N iterations of the workload's preload step and report the kernel timing")
     ap.add_argument("--gpus", type=int, default=1)

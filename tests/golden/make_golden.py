@@ -205,6 +205,25 @@ def chain_case(out, case, fields_keep=None, with_cli=True):
     print(name, "harness %.1fs cli %.1fs" % (dt, dt2), flush=True)
 
 
+def reduce_fixture(path_in, path_out, stride=8):
+    """Shrink a full-size fixture for the repository: every `stride`-th row and column of
+    each field, its full middle row and column, and its sum and sum of squares."""
+    z = np.load(path_in)
+    out = {"pa": z["pa"], "stride": np.array(stride)}
+    for k in z.files:
+        if k == "pa":
+            continue
+        a = z[k]
+        if a.ndim == 1:  # .dat files: square n x n fields
+            n = int(round(a.size ** 0.5))
+            a = a.reshape(n, n)
+        out[k + "__sub"] = a[::stride, ::stride]
+        out[k + "__midrow"] = a[a.shape[0] // 2, :]
+        out[k + "__midcol"] = a[:, a.shape[1] // 2]
+        out[k + "__sums"] = np.array([a.sum(), (a * a).sum()])
+    np.savez_compressed(path_out, **out)
+
+
 def main():
     argv = sys.argv[1:]
     out = os.path.join(ROOT, "gpurun_out", "golden")
@@ -233,6 +252,8 @@ def main():
             chain_case(out, c)
     if with_cfg2 or (only and "cfg2" in only):
         chain_case(out, CFG2, fields_keep=["P", "tauXX", "tauXY", "Ux", "Uy"], with_cli=False)
+        full = os.path.join(out, "cfg2.npz")
+        reduce_fixture(full, os.path.join(out, "cfg2_reduced.npz"))
 
 
 if __name__ == "__main__":

@@ -75,7 +75,8 @@ def check_chain(meta, z, solver, res, rtol_rec=1e-9, rtol_fields=1e-9):
         for i, key in enumerate(keys):
             a, b = res[kind][key], mod[kind][i]
             if math.isnan(b) or math.isinf(b):
-                assert (math.isnan(a) and math.isnan(b)) or a == b, (kind, key, a, b)
+                # undefined in the reference (a division by an exact zero): ours must be too
+                assert not math.isfinite(a), (kind, key, a, b)
             else:
                 assert abs(a - b) <= 1e-8 * abs(b) + 1e-300, (kind, key, a, b)
     for f in ("P", "tauXX", "tauYY", "tauXY", "Ux", "Uy"):
