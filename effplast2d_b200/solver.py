@@ -23,7 +23,7 @@ EXPORTS = (
     "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
-    "ep2d_server_stats", "ep2d_server_destroy",
+    "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc",
 )
 
 
@@ -71,6 +71,7 @@ def lib():
         L.ep2d_server_wait.argtypes = [vp, ctypes.c_uint64, i32, P(i32), P(_abi.Result), P(d), P(d)]
         L.ep2d_server_stats.argtypes = [vp, P(i64), P(i64), P(i64), P(i64), P(_abi.BatchStats)]
         L.ep2d_server_destroy.argtypes = [vp]
+        L.ep2d_average_fields_noalloc.argtypes = [i32, i32, P(d)] + [vp] * 8
         _lib = L
     return _lib
 

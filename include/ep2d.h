@@ -270,6 +270,29 @@ int ep2d_server_stats(ep2d_server* s, int64_t* submitted, int64_t* admitted, int
                       int64_t* bytes_in_use, ep2d_batch_stats* engine);
 int ep2d_server_destroy(ep2d_server* s);
 
+/* ---- scratch-free averaging ----------------------------------------------------- */
+/* No counterpart in the reference (its averaging runs on the host after copying eight
+ * fields back, EffPlast2D.cu:430-503).  For callers that cannot call cudaMalloc --
+ * code whose device memory belongs to a host framework's allocator or to a fixed pool,
+ * which a library must not grow, fragment or synchronise with cudaMalloc/cudaFree --
+ * this computes the RVE averages of fields the caller already holds in device memory
+ * and allocates nothing:
+ *   inputs, in the reference's layout, on the current device: p, tau_xx, tau_yy
+ *   (nx*ny), tau_xy ((nx-1)*(ny-1)), ux ((nx+1)*ny), uy (nx*(ny+1)); pa: pa.dat values;
+ *   out_dev[11] (caller's device memory) = sigma[0..3], sigma_per[0..3], eps_per[0..2],
+ *   divided as the reference divides them (the values ep2d_step_record holds).
+ * The reduction's partial sums use a fixed device array of 2048 x 11 doubles (176 KiB,
+ * held by every GPU that loads the library until the process exits), so ny may be at
+ * most 8194; a larger ny returns EP2D_ERR_ARG without touching the GPU.  The first call
+ * on a device looks the array's address up (cudaGetSymbolAddress) with that device
+ * current: make that first call before any stream capture.  All calls share the array,
+ * so calls that overlap on the GPU race: issue them on one stream.  The work is queued
+ * on `stream` (a cudaStream_t; NULL: the default stream) and the call returns without
+ * waiting for it. */
+int ep2d_average_fields_noalloc(int32_t nx, int32_t ny, const double pa[EP2D_NPARS], const double* p,
+                                const double* tau_xx, const double* tau_yy, const double* tau_xy,
+                                const double* ux, const double* uy, double* out_dev, void* stream);
+
 /* sizeof() of ep2d_params, ep2d_step_record, ep2d_moduli, ep2d_result, ep2d_rve_spec,
  * ep2d_batch_config and ep2d_batch_stats into out[0..n); returns the number of structs
  * (7).  Lets a binding check its layout. */
