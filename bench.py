@@ -251,7 +251,8 @@ def run_ours(args, w):
     mine = shard(world * args.steps, rank, world)
     assert len(mine) == args.steps
     # value: resident handle, each step = reset (a fresh object) + full chain
-    s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"], device=dev)
+    s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"], device=dev,
+                  kernel=args.kernel, rows=args.rows)
     res = None
     for _ in range(args.warmup):
         s.reset()
@@ -286,7 +287,7 @@ def run_ours(args, w):
     for _ in range(args.steps):
         flush.zero_()
         s2 = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
-                       device=dev)
+                       device=dev, kernel=args.kernel, rows=args.rows)
         s2.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
         s2.get("P")
         s2.get("tauXX")
@@ -358,7 +359,8 @@ def run_kernel_only(args, w):
 
     n = w["n"]
     iters = args.kernel_only
-    s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=iters, eiter=0.0, check_every=iters, device=0)
+    s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=iters, eiter=0.0, check_every=iters, device=0,
+                  kernel=args.kernel, rows=args.rows)
     s.solve_step(0, w["load"], list(w["load_type"]), 1)  # warm-up and preload
     st0 = s.stats()
     torch.cuda.synchronize()
@@ -370,7 +372,8 @@ def run_kernel_only(args, w):
     per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(st1["launches"] - st0["launches"], 1)
     bytes_alg = 64 * n * n
     peak, kind = measured_peaks()
-    print(json.dumps({"workload": args.workload, "iterations": iters, "avg_launch_us": per * 1e3,
+    print(json.dumps({"workload": args.workload, "kernel": args.kernel, "rows": args.rows,
+                      "iterations": iters, "avg_launch_us": per * 1e3,
                       "achieved_gbs": bytes_alg / (per / 1e3) / 1e9, "peak_gbs": peak, "peak_source": kind,
                       "frac": bytes_alg / (per / 1e3) / 1e9 / peak, "wall_s": wall,
                       "cell_updates_per_s": n * n / (per / 1e3)}))
@@ -444,7 +447,7 @@ def run_batch(args):
         "batched_solves_per_s": len(reqs) / t_batch, "single_fp64_solves_per_s": len(reqs) / t_single,
         "speedup": t_single / t_batch, "batched_cell_updates_per_s": cells / t_batch,
         "max_rel_moduli_error": {k: (max(v) if v else None) for k, v in errs.items()},
-        "tile_y": st["tile_y"], "tune_us": st["tune_us"], "blocks": st["blocks"],
+        "kernel": st["kernel"], "rows": st["rows"], "tune_us": st["tune_us"], "blocks": st["blocks"],
         "sides": sorted({r["n"] for r in reqs})}))
     return 0
 
@@ -489,6 +492,9 @@ def main():
     ap.add_argument("--niter", type=int, default=2_000_000, help="NITER of the batch / serve workloads")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
                     help="run N iterations of the workload's preload step and report the kernel timing")
+    ap.add_argument("--kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="iteration kernel form: 0 library's choice, 1 tile, 2 stream")
+    ap.add_argument("--rows", type=int, default=0, help="rows per tile / strip segment (0: library's choice)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)

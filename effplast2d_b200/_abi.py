@@ -23,6 +23,10 @@ ERR_NODEV = 7
 FP64 = 0
 MIXED = 1
 
+KERNEL_AUTO = 0
+KERNEL_TILE = 1
+KERNEL_STREAM = 2
+
 # field identifiers (include/ep2d.h), in the reference's array order
 FIELDS = ("P", "tauXX", "tauYY", "tauXY", "tauXYav", "J2", "J2XY",
           "Ux", "Uy", "Vx", "Vy", "K", "G")
@@ -52,6 +56,7 @@ class Params(ctypes.Structure):
         ("niter", c_int64),
         ("eiter", c_double),
         ("precision", c_int32), ("device", c_int32),
+        ("kernel", c_int32), ("rows", c_int32),
     ]
 
 
@@ -121,7 +126,7 @@ class BatchConfig(ctypes.Structure):
     _fields_ = [
         ("niter", c_int64), ("eiter", c_double),
         ("check_every", c_int32), ("precision", c_int32), ("device", c_int32),
-        ("tile_y", c_int32), ("graph_len", c_int32), ("reserved", c_int32),
+        ("rows", c_int32), ("graph_len", c_int32), ("kernel", c_int32),
     ]
 
 
@@ -129,14 +134,16 @@ class BatchStats(ctypes.Structure):
     _fields_ = [
         ("kernel_ms", c_double), ("wall_ms", c_double),
         ("launches", c_int64), ("all_launches", c_int64), ("cell_updates", c_int64),
-        ("tile_y", c_int32), ("blocks", c_int32),
-        ("tune_us", c_double * 3),
+        ("rows", c_int32), ("blocks", c_int32),
+        ("kernel", c_int32), ("n_tuned", c_int32),
+        ("tune_us", c_double * 6),
     ]
 
     def as_dict(self):
         return {"kernel_ms": self.kernel_ms, "wall_ms": self.wall_ms, "launches": self.launches,
                 "all_launches": self.all_launches, "cell_updates": self.cell_updates,
-                "tile_y": self.tile_y, "blocks": self.blocks, "tune_us": list(self.tune_us)}
+                "rows": self.rows, "blocks": self.blocks, "kernel": self.kernel,
+                "n_tuned": self.n_tuned, "tune_us": list(self.tune_us)}
 
 
 def make_spec(nx, ny, pa, nl, n_time_steps, init_load_value, load_type):
@@ -152,16 +159,17 @@ def make_spec(nx, ny, pa, nl, n_time_steps, init_load_value, load_type):
     return s
 
 
-def make_batch_config(niter=100000, eiter=1e-9, check_every=10000, precision=FP64, device=0, tile_y=0,
-                      graph_len=0):
+def make_batch_config(niter=100000, eiter=1e-9, check_every=10000, precision=FP64, device=0, rows=0,
+                      graph_len=0, kernel=0):
     c = BatchConfig()
     c.niter = int(niter)
     c.eiter = float(eiter)
     c.check_every = int(check_every)
     c.precision = int(precision)
     c.device = int(device)
-    c.tile_y = int(tile_y)
+    c.rows = int(rows)
     c.graph_len = int(graph_len)
+    c.kernel = int(kernel)
     return c
 
 
@@ -171,7 +179,7 @@ STRUCTS = {"ep2d_params": Params, "ep2d_step_record": StepRecord,
 
 
 def make_params(nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000,
-                precision=FP64, device=0):
+                precision=FP64, device=0, kernel=0, rows=0):
     p = Params()
     p.nx, p.ny = int(nx), int(ny)
     if len(pa) != NPARS:
@@ -184,4 +192,6 @@ def make_params(nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000,
     p.eiter = float(eiter)
     p.precision = int(precision)
     p.device = int(device)
+    p.kernel = int(kernel)
+    p.rows = int(rows)
     return p

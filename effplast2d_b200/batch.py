@@ -19,10 +19,11 @@ def footprint(s, precision=_abi.FP64):
     return int(lib().ep2d_rve_footprint(ctypes.byref(s), int(precision)))
 
 
-def batch_solve(specs, niter=100000, eiter=1e-9, check_every=10000, precision=_abi.FP64, device=0, tile_y=0,
-                graph_len=0):
-    """Solve every spec together; returns (list of result dicts, stats dict)."""
-    cfg = _abi.make_batch_config(niter, eiter, check_every, precision, device, tile_y, graph_len)
+def batch_solve(specs, niter=100000, eiter=1e-9, check_every=10000, precision=_abi.FP64, device=0, rows=0,
+                graph_len=0, kernel=_abi.KERNEL_AUTO):
+    """Solve every spec together; returns (list of result dicts, stats dict).  rows = 0
+    lets the library time the kernel forms and rows on the first launches."""
+    cfg = _abi.make_batch_config(niter, eiter, check_every, precision, device, rows, graph_len, kernel)
     n = len(specs)
     arr = (_abi.RveSpec * n)(*specs)
     res = (_abi.Result * n)()
@@ -38,8 +39,8 @@ class Server:
     latency measured from submission."""
 
     def __init__(self, mem_budget_bytes, max_active=0, niter=100000, eiter=1e-9, check_every=10000,
-                 precision=_abi.FP64, device=0, tile_y=0, graph_len=0):
-        self.cfg = _abi.make_batch_config(niter, eiter, check_every, precision, device, tile_y, graph_len)
+                 precision=_abi.FP64, device=0, rows=0, graph_len=0, kernel=_abi.KERNEL_AUTO):
+        self.cfg = _abi.make_batch_config(niter, eiter, check_every, precision, device, rows, graph_len, kernel)
         h = ctypes.c_void_p()
         _check(lib().ep2d_server_create(ctypes.byref(self.cfg), int(mem_budget_bytes), int(max_active),
                                         ctypes.byref(h)))

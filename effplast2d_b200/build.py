@@ -21,7 +21,7 @@ CUDA_INC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include
 
 CU_SOURCES = ["ep2d_kernels.cu", "ep2d_noalloc.cu"]
 CPP_SOURCES = ["ep2d_rve.cpp", "ep2d_api.cpp", "ep2d_batch.cpp"]
-HEADERS = ["ep2d_device.cuh", "ep2d_iter_f64.cuh", "ep2d_types.hpp", "ep2d_rve.hpp", "ep2d_batch.hpp"]
+HEADERS = ["ep2d_device.cuh", "ep2d_stencil.cuh", "ep2d_iter_f64.cuh", "ep2d_iter_stream.cuh", "ep2d_types.hpp", "ep2d_rve.hpp", "ep2d_batch.hpp"]
 
 
 def _newer(target, deps):

@@ -42,8 +42,14 @@ int validate_config(const ep2d_batch_config& c) {
   if (c.niter < c.check_every || c.niter % c.check_every != 0)
     return fail(EP2D_ERR_ARG, "niter must be a positive multiple of check_every in a batch");
   if (c.precision != EP2D_FP64 && c.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
-  if (c.tile_y != 0 && c.tile_y != 8 && c.tile_y != 16 && c.tile_y != 32)
-    return fail(EP2D_ERR_ARG, "tile_y must be 0, 8, 16 or 32");
+  if (c.kernel < EP2D_KERNEL_AUTO || c.kernel > EP2D_KERNEL_STREAM) return fail(EP2D_ERR_ARG, "unknown kernel form");
+  if (c.rows != 0) {
+    IterShape sh;
+    sh.form = c.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
+    sh.rows = c.rows;
+    if (!shape_valid(sh))
+      return fail(EP2D_ERR_ARG, "rows must be 0, or 8, 16 or 32 for the tile form and 16..1024 for the stream form");
+  }
   if (c.graph_len < 0 || (c.graph_len % 2) != 0) return fail(EP2D_ERR_ARG, "graph_len must be even");
   return EP2D_OK;
 }
@@ -85,13 +91,22 @@ int BatchEngine::init(const ep2d_batch_config& c) {
   EP2D_CK(cudaEventCreate(&ev_[0]));
   EP2D_CK(cudaEventCreate(&ev_[1]));
   EP2D_CK(cudaMalloc(&d_ntiles_, sizeof(int)));
-  tile_y = c.tile_y ? c.tile_y : TILE_Y;
-  tuned = c.tile_y != 0;
-  blocks = sm_count_ * iter_blocks_per_sm(false, c.precision == EP2D_MIXED, tile_y);
+  shape.form = c.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
+  shape.rows = c.rows ? c.rows : (shape.form == FORM_TILE ? TILE_Y : SEG_DEFAULT);
+  tuned = c.rows != 0;
+  blocks = sm_count_ * iter_blocks_per_sm(false, c.precision == EP2D_MIXED, shape);
   return grow(16);
 }
 
 size_t BatchEngine::footprint(const ep2d_rve_spec& s) const { return Rve::footprint(params_of(cfg, s)); }
+
+void BatchEngine::fill_stats(ep2d_batch_stats* st) const {
+  st->rows = shape.rows;
+  st->blocks = blocks;
+  st->kernel = shape.form == FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;
+  st->n_tuned = n_tuned;
+  for (int q = 0; q < 6; q++) st->tune_us[q] = tune_us[q];
+}
 
 int BatchEngine::grow(int need) {
   if (need <= cap_slots_) return EP2D_OK;
@@ -159,7 +174,7 @@ int BatchEngine::add(const ep2d_rve_spec& spec, uint64_t ticket, double submit_s
     s.rve.reset();
     return rc;
   }
-  s.rve->tile_y = tile_y;
+  s.rve->shape = shape;
   s.used = true;
   s.task = Task{};
   s.task.spec = spec;
@@ -184,7 +199,8 @@ int BatchEngine::rebuild_tiles() {
   for (size_t k = 0; k < slots_.size(); k++) {
     const Slot& s = slots_[k];
     if (!s.used || s.task.done) continue;
-    const int tx = (s.rve->g.nx + TILE_X - 1) / TILE_X, ty = (s.rve->g.ny + tile_y - 1) / tile_y;
+    int tx = 0, ty = 0;
+    shape_units(shape, s.rve->g.nx, s.rve->g.ny, &tx, &ty);
     for (int by = 0; by < ty; by++)
       for (int bx = 0; bx < tx; bx++) tiles.push_back(make_int2((int)k, bx | (by << 16)));
   }
@@ -210,7 +226,7 @@ int BatchEngine::rebuild_tiles() {
 }
 
 int BatchEngine::ensure_graph() {
-  if (graph_ && graph_tile_y_ == tile_y) return EP2D_OK;
+  if (graph_ && graph_shape_.form == shape.form && graph_shape_.rows == shape.rows) return EP2D_OK;
   if (graph_) {
     cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
@@ -220,7 +236,7 @@ int BatchEngine::ensure_graph() {
   EP2D_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < cfg.graph_len && le == cudaSuccess; k++)
-    le = launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, k & 1, false, mixed, tile_y, blocks, stream);
+    le = launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, k & 1, false, mixed, shape, blocks, stream);
   const cudaError_t ee = cudaStreamEndCapture(stream, &g);
   if (le != cudaSuccess || ee != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
@@ -229,7 +245,7 @@ int BatchEngine::ensure_graph() {
   const cudaError_t ie = cudaGraphInstantiate(&graph_, g, 0);
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
-  graph_tile_y_ = tile_y;
+  graph_shape_ = shape;
   return EP2D_OK;
 }
 
@@ -243,7 +259,7 @@ int BatchEngine::launch_plain_run(int64_t k0, int64_t n) {
       k += cfg.graph_len;
       n -= cfg.graph_len;
     } else {
-      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(k & 1), false, mixed, tile_y, blocks, stream));
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(k & 1), false, mixed, shape, blocks, stream));
       k++;
       n--;
     }
@@ -251,44 +267,60 @@ int BatchEngine::launch_plain_run(int64_t k0, int64_t n) {
   return EP2D_OK;
 }
 
-// Time the tile heights on real iterations of the first interval (they advance the
-// solution like any other launch) and keep the fastest.  *k: launches done so far.
+// Time the candidate kernel shapes (tile form, rows 8/16/32; stream form, rows
+// 32/64/128; only the form cfg.kernel names unless it is AUTO) on real iterations of
+// the first interval -- they advance the solution like any other launch -- and keep
+// the fastest.  *k: launches done so far.
 int BatchEngine::autotune(int64_t* k, int64_t n_avail) {
-  const int cand[3] = {16, 8, 32};
+  IterShape cand[6];
+  int slot[6], nc = 0;
+  if (cfg.kernel != EP2D_KERNEL_TILE)
+    for (int q = 0; q < 3; q++) {
+      cand[nc].form = FORM_STREAM;
+      cand[nc].rows = SEG_CHOICES[q];
+      slot[nc++] = 3 + q;
+    }
+  if (cfg.kernel != EP2D_KERNEL_STREAM)
+    for (int q = 0; q < 3; q++) {
+      cand[nc].form = FORM_TILE;
+      cand[nc].rows = TILE_Y_CHOICES[q];
+      slot[nc++] = q;
+    }
   const int per = 24;  // 4 warm-up + 20 timed launches per candidate
-  if (n_avail < 3 * per) {
+  if (n_avail < nc * per) {
     tuned = true;
     return EP2D_OK;
   }
   const bool mixed = cfg.precision == EP2D_MIXED;
   float best = 1e30f;
-  int best_ty = tile_y;
-  for (int c = 0; c < 3; c++) {
-    tile_y = cand[c];
-    blocks = sm_count_ * iter_blocks_per_sm(false, mixed, tile_y);
+  IterShape best_shape = shape;
+  for (int c = 0; c < nc; c++) {
+    shape = cand[c];
+    blocks = sm_count_ * iter_blocks_per_sm(false, mixed, shape);
     int rc = rebuild_tiles();
     if (rc) return rc;
     for (int w = 0; w < 4; w++, (*k)++)
-      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, tile_y, blocks, stream));
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, shape, blocks, stream));
     EP2D_CK(cudaEventRecord(ev_[0], stream));
     for (int w = 0; w < per - 4; w++, (*k)++)
-      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, tile_y, blocks, stream));
+      EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)(*k & 1), false, mixed, shape, blocks, stream));
     EP2D_CK(cudaEventRecord(ev_[1], stream));
     EP2D_CK(cudaEventSynchronize(ev_[1]));
     float ms = 0.0f;
     EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     kernel_ms += ms;
     const float us = 1000.0f * ms / (per - 4);
-    tune_us[tile_y == 8 ? 0 : (tile_y == 16 ? 1 : 2)] = us;
+    tune_us[slot[c]] = us;
+    n_tuned++;
     if (us < best) {
       best = us;
-      best_ty = tile_y;
+      best_shape = shape;
     }
   }
-  tile_y = best_ty;
-  blocks = sm_count_ * iter_blocks_per_sm(false, mixed, tile_y);
+  shape = best_shape;
+  blocks = sm_count_ * iter_blocks_per_sm(false, mixed, shape);
   for (auto& s : slots_)
-    if (s.used) s.rve->tile_y = tile_y;
+    if (s.used) s.rve->shape = shape;
   tuned = true;
   return rebuild_tiles();
 }
@@ -363,7 +395,7 @@ int BatchEngine::run_interval() {
   rc = launch_plain_run(k, ce - 1 - k);
   if (rc) return rc;
   EP2D_CK(cudaMemsetAsync(d_vmax_, 0, slots_.size() * 2 * sizeof(unsigned long long), stream));
-  EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)((ce - 1) & 1), true, mixed, tile_y, blocks, stream));
+  EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)((ce - 1) & 1), true, mixed, shape, blocks, stream));
   EP2D_CK(cudaEventRecord(ev_[1], stream));
   EP2D_CK(cudaMemcpyAsync(h_vmax_, d_vmax_, slots_.size() * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           stream));
@@ -517,9 +549,7 @@ class Server {
         stats_snapshot_.launches = eng_.launches;
         stats_snapshot_.all_launches = eng_.launches + eng_.aux_launches;
         stats_snapshot_.cell_updates = eng_.cell_updates;
-        stats_snapshot_.tile_y = eng_.tile_y;
-        stats_snapshot_.blocks = eng_.blocks;
-        for (int q = 0; q < 3; q++) stats_snapshot_.tune_us[q] = eng_.tune_us[q];
+        eng_.fill_stats(&stats_snapshot_);
       }
       if (!fin.empty()) cv_.notify_all();
     }
@@ -608,9 +638,7 @@ int ep2d_batch_solve(const ep2d_batch_config* cfg, const ep2d_rve_spec* specs, i
       stats->launches = eng.launches;
       stats->all_launches = eng.launches + eng.aux_launches;
       stats->cell_updates = eng.cell_updates;
-      stats->tile_y = eng.tile_y;
-      stats->blocks = eng.blocks;
-      for (int q = 0; q < 3; q++) stats->tune_us[q] = eng.tune_us[q];
+      eng.fill_stats(stats);
     }
     return status ? fail(status, "a batch member failed") : EP2D_OK;
   } catch (const std::exception& ex) {

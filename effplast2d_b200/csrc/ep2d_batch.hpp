@@ -58,9 +58,12 @@ class BatchEngine {
   // statistics
   double kernel_ms = 0.0;
   int64_t launches = 0, aux_launches = 0, cell_updates = 0;
-  int tile_y = 0, blocks = 0;
+  IterShape shape{};  // kernel form and rows of the batched launches
+  int blocks = 0;
   bool tuned = false;
-  double tune_us[3] = {0, 0, 0};
+  int n_tuned = 0;
+  double tune_us[6] = {0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 32/64/128
+  void fill_stats(ep2d_batch_stats* st) const;
 
  private:
   struct Slot {
@@ -70,7 +73,7 @@ class BatchEngine {
   };
   int begin_task_step(Slot& s);
   int advance(Slot& s, double error);  // after a checkpoint of this slot's time step
-  int rebuild_tiles();
+  int rebuild_tiles();  // the work list: tiles or strip segments of every active RVE
   int ensure_graph();
   int launch_plain_run(int64_t k0, int64_t n);
   int autotune(int64_t* k, int64_t n_avail);
@@ -88,7 +91,7 @@ class BatchEngine {
   unsigned long long* h_vmax_ = nullptr;
   int cap_slots_ = 0, cap_tiles_ = 0;
   cudaGraphExec_t graph_ = nullptr;
-  int graph_tile_y_ = 0;
+  IterShape graph_shape_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
   int sm_count_ = 148;
 };

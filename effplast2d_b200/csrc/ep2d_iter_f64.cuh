@@ -20,12 +20,11 @@
 // Arithmetic: displacements and all arithmetic are FP64; velocities are stored as TV
 // (double on the plain path, float on the mixed path: velocities only scale the next
 // displacement increment, so their FP32 rounding is relative to a quantity that goes
-// to zero and leaves no floor on the convergence test).  Divisions by dX, dY, 3 and
-// rho are multiplications by host-computed reciprocals, and the yield test compares
-// J2^2 with coh^2 so that the square root and the division by J2 run only in yielding
-// cells.  Results differ from the reference's division/sqrt forms by rounding only.
+// to zero and leaves no floor on the convergence test).  The per-cell formulas are
+// those of ep2d_stencil.cuh, shared with the stream form, so both forms round alike.
 #pragma once
 
+#include "ep2d_stencil.cuh"
 #include "ep2d_types.hpp"
 
 namespace ep2d {
@@ -98,6 +97,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
 
   const double rdX = g.rdX, rdY = g.rdY;
   const double third = 1.0 / 3.0;
+  const double G20 = __dmul_rn(2.0, g.G0), G2p = __dmul_rn(2.0, g.Gp);
   // ---- B: trial stresses at nodes (i0-1+li, j0-1+lj) and corners (i0-2+li, j0-2+lj)
 #pragma unroll
   for (int lj = ty; lj < SH; lj += 8) {
@@ -108,16 +108,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
         double pv = 0.0, xv = 0.0, yv = 0.0;
         if (i >= 0 && i < nx && j >= 0 && j < ny) {
           const uint8_t m = s.m[lj + 1][li + 1];
-          const double K = (m & M_MAT) ? g.Kp : g.K0;
-          const double G2 = 2.0 * ((m & M_MAT) ? g.Gp : g.G0);
-          const double exx = (s.ux[lj + 1][li + 1] - s.ux[lj + 1][li]) * rdX;
-          const double eyy = (s.uy[lj + 1][li + 1] - s.uy[lj][li + 1]) * rdY;
-          const double divU = exx + eyy;
-          if (!(m & M_NODE)) {
-            pv = -K * divU;
-            xv = G2 * (exx - divU * third);
-            yv = G2 * (eyy - divU * third);
-          }
+          if (!(m & M_NODE))
+            node_trial(__dsub_rn(s.ux[lj + 1][li + 1], s.ux[lj + 1][li]), __dsub_rn(s.uy[lj + 1][li + 1], s.uy[lj][li + 1]),
+                       (m & M_MAT) ? g.Kp : g.K0, (m & M_MAT) ? G2p : G20, rdX, rdY, third, pv, xv, yv);
         }
         s.p[lj][li] = pv;
         s.xx[lj][li] = xv;
@@ -128,11 +121,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
         double t = 0.0;
         if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
           const uint8_t m00 = s.m[lj][li], m10 = s.m[lj][li + 1], m01 = s.m[lj + 1][li], m11 = s.m[lj + 1][li + 1];
-          if (!(m00 & M_CORNER)) {
-            const double Gs = ((m00 & M_MAT) ? g.Gp : g.G0) + ((m10 & M_MAT) ? g.Gp : g.G0) +
-                              ((m01 & M_MAT) ? g.Gp : g.G0) + ((m11 & M_MAT) ? g.Gp : g.G0);
-            t = 0.25 * Gs * ((s.ux[lj + 1][li] - s.ux[lj][li]) * rdY + (s.uy[lj][li + 1] - s.uy[lj][li]) * rdX);
-          }
+          if (!(m00 & M_CORNER))
+            t = corner_trial(corner_g4(m00, m10, m01, m11, g.G0, g.Gp), __dsub_rn(s.ux[lj + 1][li], s.ux[lj][li]),
+                             __dsub_rn(s.uy[lj][li + 1], s.uy[lj][li]), rdX, rdY);
         }
         s.xy[lj][li] = t;
       }
@@ -152,21 +143,15 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
           double fn = 1.0;
           if (i >= 0 && i < nx && j >= 0 && j < ny) {
             const int a = min(max(i - 1, 0), nx - 3) - (i0 - 2), b = min(max(j - 1, 0), ny - 3) - (j0 - 2);
-            const double tav = 0.25 * (s.xy[b][a] + s.xy[b][a + 1] + s.xy[b + 1][a] + s.xy[b + 1][a + 1]);
+            const double tav = __dmul_rn(
+                0.25, __dadd_rn(__dadd_rn(__dadd_rn(s.xy[b][a], s.xy[b][a + 1]), s.xy[b + 1][a]), s.xy[b + 1][a + 1]));
             const double xv = s.xx[lj][li], yv = s.yy[lj][li];
-            const double J2sq = xv * xv + yv * yv + 2.0 * tav * tav;
-            double J2 = 0.0;
-            if (J2sq > coh2) {
-              J2 = sqrt(J2sq);
-              fn = coh / J2;
-            }
+            const double J2sq = node_j2sq(xv, yv, tav);
+            fn = return_factor(J2sq, coh, coh2);
             if (RECORD && li >= 1 && lj >= 1) {
-              double tavo = tav, J2o = (J2sq > coh2) ? J2 : sqrt(J2sq);
-              if (fn != 1.0) {
-                const double xo = xv * fn, yo = yv * fn;
-                tavo = tav * fn;
-                J2o = sqrt(xo * xo + yo * yo + 2.0 * tavo * tavo);
-              }
+              const double tavo = __dmul_rn(tav, fn);
+              const double J2o =
+                  (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xv, fn), __dmul_rn(yv, fn), tavo)) : __dsqrt_rn(J2sq);
               f.txyav[j * pitch + i] = tavo;
               f.j2[j * pitch + i] = J2o;
             }
@@ -177,12 +162,13 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
           const int ci = i0 - 1 + li, cj = j0 - 1 + lj;
           double fc = 1.0;
           if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
-            const double sx = s.xx[lj][li] + s.xx[lj][li + 1] + s.xx[lj + 1][li] + s.xx[lj + 1][li + 1];
-            const double sy = s.yy[lj][li] + s.yy[lj][li + 1] + s.yy[lj + 1][li] + s.yy[lj + 1][li + 1];
-            const double t = s.xy[lj + 1][li + 1];
-            const double J2sq = 0.0625 * sx * sx + 0.0625 * sy * sy + 2.0 * t * t;
-            if (J2sq > coh2) fc = coh / sqrt(J2sq);
-            if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = sqrt(J2sq);
+            const double sx =
+                __dadd_rn(__dadd_rn(__dadd_rn(s.xx[lj][li], s.xx[lj][li + 1]), s.xx[lj + 1][li]), s.xx[lj + 1][li + 1]);
+            const double sy =
+                __dadd_rn(__dadd_rn(__dadd_rn(s.yy[lj][li], s.yy[lj][li + 1]), s.yy[lj + 1][li]), s.yy[lj + 1][li + 1]);
+            const double J2sq = corner_j2sq(sx, sy, s.xy[lj + 1][li + 1]);
+            fc = return_factor(J2sq, coh, coh2);
+            if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = __dsqrt_rn(J2sq);
           }
           s.fc[lj][li] = fc;
         }
@@ -194,9 +180,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
 #pragma unroll
       for (int li = tx; li < FW; li += 32) {
         const double fn = s.fn[lj][li];
-        s.xx[lj][li] *= fn;
-        s.yy[lj][li] *= fn;
-        s.xy[lj + 1][li + 1] *= s.fc[lj][li];
+        s.xx[lj][li] = __dmul_rn(s.xx[lj][li], fn);
+        s.yy[lj][li] = __dmul_rn(s.yy[lj][li], fn);
+        s.xy[lj + 1][li + 1] = __dmul_rn(s.xy[lj + 1][li + 1], s.fc[lj][li]);
       }
     }
     __syncthreads();
@@ -213,22 +199,22 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
     const size_t q = j * pitch + i;
     double vx = vxr[r];
     if (i > 0 && j > 0 && j < ny - 1) {
-      vx = vx * cX + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj + 1][li] + s.xx[lj + 1][li + 1] - s.xx[lj + 1][li]) * rdX +
-                            (s.xy[lj + 2][li + 1] - s.xy[lj + 1][li + 1]) * rdY);
+      vx = face_velocity(vx, cX, dtr, face_diff(s.p[lj + 1][li + 1], s.p[lj + 1][li], s.xx[lj + 1][li + 1], s.xx[lj + 1][li]),
+                         rdX, __dsub_rn(s.xy[lj + 2][li + 1], s.xy[lj + 1][li + 1]), rdY);
       const TV vs = (TV)vx;
       fvx[q] = vs;
       vx = (double)vs;  // the displacement moves by the stored velocity
     }
-    uxo[q] = s.ux[lj + 2][li + 1] + vx * dT;
+    uxo[q] = advance(s.ux[lj + 2][li + 1], vx, dT);
     double vy = vyr[r];
     if (i > 0 && i < nx - 1 && j > 0) {
-      vy = vy * cY + dtr * ((-s.p[lj + 1][li + 1] + s.p[lj][li + 1] + s.yy[lj + 1][li + 1] - s.yy[lj][li + 1]) * rdY +
-                            (s.xy[lj + 1][li + 2] - s.xy[lj + 1][li + 1]) * rdX);
+      vy = face_velocity(vy, cY, dtr, face_diff(s.p[lj + 1][li + 1], s.p[lj][li + 1], s.yy[lj + 1][li + 1], s.yy[lj][li + 1]),
+                         rdY, __dsub_rn(s.xy[lj + 1][li + 2], s.xy[lj + 1][li + 1]), rdX);
       const TV vs = (TV)vy;
       fvy[q] = vs;
       vy = (double)vs;
     }
-    uyo[q] = s.uy[lj + 1][li + 2] + vy * dT;
+    uyo[q] = advance(s.uy[lj + 1][li + 2], vy, dT);
     if (i == nx - 1) {  // face column i = nx of Ux/Vx: never updated by the reference
       const size_t q2 = j * pitch + nx;
       uxo[q2] = s.ux[lj + 2][li + 2];

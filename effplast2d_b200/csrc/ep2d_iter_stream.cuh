@@ -1,0 +1,366 @@
+// ep2d_iter_stream.cuh -- the fused iteration kernel, column-streaming form.
+//
+// Same iteration as ep2d_iter_f64.cuh (ComputeStress -> ComputeJ2 -> ComputePlasticity
+// -> ComputeDisp, EffPlast2D.cu:3-177), same per-cell formulas (ep2d_stencil.cuh), a
+// different mapping.  A warp owns 28 columns (lanes 2..29; lanes 0, 1, 30, 31 are
+// halo) and a segment of rows; each lane keeps its column's values of the last few rows
+// in registers and the warp marches up its segment one row per step.  At step r a lane
+//   takes   Ux, Uy, Vx, Vy and the mask of row r+1 from its shared-memory ring,
+//   forms   the trial stresses of row r (node and corner),
+//   returns row r-1 (node: tauXY averaged onto the node from the clamped 2x2 corner
+//           block; corner: tauXX, tauYY averaged onto the corner),
+//   updates the faces of row r-1 (damped momentum, U += V dt).
+// Rows reach the ring by cp.async, STREAM_DEPTH rows ahead of use, so each warp keeps
+// that many rows of loads in flight without holding them in registers: the march is a
+// chain of dependent steps, and without the ring a warp would wait one memory latency
+// per row.  Neighbouring columns come from warp shuffles; a value a step needs from a
+// neighbour that the previous step already fetched (the same quantity one row lower)
+// is carried in a register instead of fetched again.  There is no block-wide barrier;
+// each lane reads only the ring entries it wrote.
+//
+// Segments whose 32 columns and rows jA-3 .. jB+1 lie inside the grid away from its
+// edges run the INTERIOR instantiation: no bounds tests, and the clamped 2x2 corner
+// block of the node return is always the one below-left.  Segments touching an edge
+// run the general one.  Both call the same formulas, so they round alike.
+#pragma once
+
+#include "ep2d_stencil.cuh"
+#include "ep2d_types.hpp"
+
+namespace ep2d {
+
+constexpr int STREAM_COLS = 28;                 // owned columns per warp
+constexpr int STREAM_WARPS = 4;                 // warps per CTA
+constexpr int STREAM_DEPTH = 8;                 // rows of loads in flight per warp
+constexpr int STREAM_SLOTS = STREAM_DEPTH + 1;  // the slot refilled was read one step earlier
+
+// One row of a warp's 32 columns, as the ring holds it; m: the aligned 32-bit word of
+// the byte mask that contains the lane's node.
+template <typename TV>
+struct StreamRow {
+  double ux[32];
+  double uy[32];
+  TV vx[32];
+  TV vy[32];
+  uint32_t m[32];
+};
+
+// Shared memory of one warp: its ring, then the 16-entry table of corner_g4 by the
+// material bits of the four nodes around a corner.
+template <typename TV>
+struct StreamWarpSmem {
+  StreamRow<TV> ring[STREAM_SLOTS];
+  double g4[16];
+};
+
+template <typename TV>
+constexpr size_t stream_smem_bytes() {
+  return sizeof(StreamWarpSmem<TV>) * STREAM_WARPS;
+}
+
+__device__ __forceinline__ double shfl_idx(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double shfl_dn(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ int shfl_dn_i(int v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// cp.async of 4 or 8 bytes; with ok == false nothing is read and the destination is
+// zero-filled (src-size 0), `src` then only has to be a valid address.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, bool ok) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES), "r"(ok ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// true if segment (strip, jA..jB) may run the INTERIOR instantiation: every lane's
+// column in [0, nx-1] and at least one column from the right edge, rows jA-3 .. jB+1
+// inside the grid with jB <= ny-2
+__device__ __forceinline__ bool stream_interior(int nx, int ny, int strip, int jA, int jB) {
+  return strip >= 1 && STREAM_COLS * strip + 29 <= nx - 3 && jA >= 3 && jB <= ny - 2;
+}
+
+template <bool PLASTIC, bool RECORD, bool INTERIOR, typename TV>
+__device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const int src, const int strip,
+                                            const int jA, const int jB, StreamWarpSmem<TV>& sm, double& vmx,
+                                            double& vmy) {
+  const int lane = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny;
+  const int pitch = g.pitch;  // pitch * (ny + 1) < 2^31 (checked on the host)
+  const int i = STREAM_COLS * strip - 2 + lane;
+  const bool own = INTERIOR ? (lane >= 2 && lane < 2 + STREAM_COLS) : (lane >= 2 && lane < 2 + STREAM_COLS && i < nx);
+  const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
+  const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
+  double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
+  double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
+  TV* __restrict__ fvx = static_cast<TV*>(f.vx);
+  TV* __restrict__ fvy = static_cast<TV*>(f.vy);
+  const uint8_t* __restrict__ mask = f.mask;
+
+  const bool colx = INTERIOR || (i >= 0 && i <= nx);  // column of Ux / Vx
+  const bool coln = INTERIOR || (i >= 0 && i < nx);   // column of nodes, Uy, Vy
+  const int mshift = 8 * (i & 3);                     // pitch % 32 == 0: byte i & 3 of the word
+
+  // rows k_first .. k_last pass through the ring: U and the mask are needed up to row
+  // r + 1 and V up to row r for steps r = jA - 2 .. jB
+  const int k_first = jA - 3, k_last = jB + 1;
+  auto issue = [&](int k, int slot) {
+    StreamRow<TV>& row = sm.ring[slot];
+    const bool rx = INTERIOR || (colx && k >= 0 && k < ny);   // Ux, Vx: rows 0 .. ny-1
+    const bool ry = INTERIOR || (coln && k >= 0 && k <= ny);  // Uy, Vy: rows 0 .. ny
+    const bool rm = INTERIOR || (coln && k >= 0 && k < ny);   // nodes
+    const int q = (rx || ry) ? k * pitch + i : 0;
+    cp_async_zfill<8>(&row.ux[lane], ux + (rx ? q : 0), rx);
+    cp_async_zfill<8>(&row.uy[lane], uy + (ry ? q : 0), ry);
+    cp_async_zfill<(int)sizeof(TV)>(&row.vx[lane], fvx + (rx ? q : 0), rx);
+    cp_async_zfill<(int)sizeof(TV)>(&row.vy[lane], fvy + (ry ? q : 0), ry);
+    cp_async_zfill<4>(&row.m[lane], mask + (rm ? (q & ~3) : 0), rm);
+  };
+  int slot_rd = 0, slot_wr = 0;
+#pragma unroll 1
+  for (int d = 0; d < STREAM_DEPTH; d++) {
+    if (k_first + d <= k_last) issue(k_first + d, slot_wr);
+    cp_async_commit();  // empty groups keep the count uniform
+    slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
+  }
+
+  const double rdX = g.rdX, rdY = g.rdY, third = 1.0 / 3.0;
+  const double coh = g.coh, coh2 = g.coh2;
+  const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
+  const double K0 = g.K0, Kp = g.Kp, G0 = g.G0, Gp = g.Gp;
+  const double G20 = __dmul_rn(2.0, G0), G2p = __dmul_rn(2.0, Gp);
+  __syncwarp();  // the previous segment of this warp has stopped reading the table
+  if (lane < 16) sm.g4[lane] = corner_g4_of_bits(lane, G0, Gp);
+  __syncwarp();
+
+  // windows at step r: U rows r-1 (m), r (0), r+1 (p); masks rows r, r+1; V rows r-1,
+  // r, r+1 (m, 0, n).  Suffix _r: the value of the lane to the right (column i+1),
+  // _l: to the left (column i-1).
+  double uxm = 0.0, ux0 = 0.0, uxp = 0.0, uym = 0.0, uy0 = 0.0, uyp = 0.0;
+  double uxp_r = 0.0;  // Ux(i+1, r+1); at the next step Ux(i+1, r)
+  int mk0 = 0, mkp = 0, mkp_r = 0;
+  double vxm = 0.0, vx0 = 0.0, vxn = 0.0, vym = 0.0, vy0 = 0.0, vyn = 0.0;
+  // trial stresses: nodes rows r-1 (a) and r (b); corners rows r-3..r (c0..c3)
+  double xa = 0.0, ya = 0.0, pb = 0.0, xb = 0.0, yb = 0.0, pa_ = 0.0;
+  double xb_r = 0.0, yb_r = 0.0;  // node trial row r of column i+1; next step: row r-1
+  double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
+  double c2_l = 0.0;  // corner trial row r-1 of column i-1; next step: row r-2
+  // returned stresses: nodes rows r-2 (q) and r-1 (w); corners rows r-2 (cq), r-1 (cw)
+  double pq = 0.0, yq = 0.0, pw = 0.0, xw = 0.0, yw = 0.0, cq = 0.0, cw = 0.0;
+  double cw_l = 0.0;  // returned corner row r-1 of column i-1; next step: row r-2
+
+  double ux0_r = 0.0;  // Ux(i+1, r)
+  int mk0_r = 0;
+  int g_lo = 0, g_hi = 0;  // material bits of nodes (i, i+1) in rows r and r+1
+  int k = k_first;
+  // bring row k from the ring into the windows and refill the ring
+  auto take_row = [&]() {
+    cp_async_wait<STREAM_DEPTH - 1>();  // row k has landed
+    ux0_r = uxp_r;
+    mk0_r = mkp_r;
+    {
+      const StreamRow<TV>& row = sm.ring[slot_rd];
+      uxm = ux0; ux0 = uxp; uxp = row.ux[lane];
+      uym = uy0; uy0 = uyp; uyp = row.uy[lane];
+      mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
+      vxm = vx0; vx0 = vxn; vxn = (double)row.vx[lane];
+      vym = vy0; vy0 = vyn; vyn = (double)row.vy[lane];
+    }
+    slot_rd = (slot_rd + 1 == STREAM_SLOTS) ? 0 : slot_rd + 1;
+    if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr);
+    cp_async_commit();
+    slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
+    uxp_r = shfl_dn(uxp);
+    mkp_r = shfl_dn_i(mkp);
+    g_lo = g_hi;
+    g_hi = (mkp & M_MAT) | ((mkp_r & M_MAT) << 1);
+  };
+  take_row();  // rows k_first and k_first + 1 only fill the windows
+  k++;
+  take_row();
+  k++;
+#pragma unroll 2
+  for (; k <= k_last; k++) {
+    take_row();
+    const int r = k - 1;
+
+    // ---- trial stresses of row r
+    const double uyp_r = shfl_dn(uyp);
+    double pn = 0.0, xn = 0.0, yn = 0.0, cn = 0.0;
+    if ((INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE))
+      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), (mk0 & M_MAT) ? Kp : K0, (mk0 & M_MAT) ? G2p : G20, rdX,
+                 rdY, third, pn, xn, yn);
+    if ((INTERIOR || (i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1)) && !(mk0 & M_CORNER))
+      cn = corner_trial(sm.g4[g_lo | (g_hi << 2)], __dsub_rn(uxp_r, ux0_r), __dsub_rn(uyp_r, uyp), rdX, rdY);
+    const double xa_r = xb_r, ya_r = yb_r;
+    pa_ = pb; xa = xb; ya = yb;
+    pb = pn; xb = xn; yb = yn;
+    xb_r = shfl_dn(xb);
+    yb_r = shfl_dn(yb);
+    const double c1_l = c2_l;
+    c0 = c1; c1 = c2; c2 = c3; c3 = cn;
+    c2_l = shfl_up1(c2);
+
+    // ---- return of row j = r - 1
+    const int j = r - 1;
+    double xr = xa, yr = ya, cr = c2;
+    double tav_o = 0.0, j2_o = 0.0, j2xy_o = 0.0;
+    if (PLASTIC) {
+      // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
+      double c00, c10, c01, c11;
+      if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j)
+        c00 = c1_l; c10 = c1; c01 = c2_l; c11 = c2;
+      } else {
+        const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
+        const int bsel = min(max(j - 1, 0), ny - 3) - j;
+        const double cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
+        const double cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
+        const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
+        c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
+        c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
+      }
+      double fn = 1.0, fc = 1.0;
+      if (INTERIOR || (coln && j >= 0 && j < ny)) {
+        const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
+        const double J2sq = node_j2sq(xa, ya, tav);
+        fn = return_factor(J2sq, coh, coh2);
+        if (RECORD) {
+          tav_o = __dmul_rn(tav, fn);
+          j2_o = (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o)) : __dsqrt_rn(J2sq);
+        }
+      }
+      // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
+      if (INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1)) {
+        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
+        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
+        const double J2sq = corner_j2sq(sx, sy, c2);
+        fc = return_factor(J2sq, coh, coh2);
+        if (RECORD) j2xy_o = __dsqrt_rn(J2sq);
+      }
+      xr = __dmul_rn(xa, fn);
+      yr = __dmul_rn(ya, fn);
+      cr = __dmul_rn(c2, fc);
+    }
+    const double cq_l = cw_l;
+    pq = pw; yq = yw; cq = cw;
+    pw = pa_; xw = xr; yw = yr; cw = cr;
+    cw_l = shfl_up1(cw);
+
+    // ---- faces of row j (owned rows [jA, jB))
+    const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
+    double uxm_r = 0.0, vxm_r = 0.0;
+    if (!INTERIOR) {
+      uxm_r = shfl_dn(uxm);
+      vxm_r = shfl_dn(vxm);
+    }
+    if (j >= jA && own) {
+      const int q = j * pitch + i;
+      double vx = vxm;
+      if (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) {
+        vx = face_velocity(vx, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, __dsub_rn(cw_l, cq_l), rdY);
+        const TV vs = (TV)vx;
+        fvx[q] = vs;
+        vx = (double)vs;  // the displacement moves by the stored velocity
+      }
+      uxo[q] = advance(uxm, vx, dT);
+      double vy = vym;
+      if (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) {
+        vy = face_velocity(vy, cY, dtr, face_diff(pw, pq, yw, yq), rdY, __dsub_rn(cq, cq_l), rdX);
+        const TV vs = (TV)vy;
+        fvy[q] = vs;
+        vy = (double)vs;
+      }
+      uyo[q] = advance(uym, vy, dT);
+      if (!INTERIOR) {
+        if (i == nx - 1) {  // face column nx of Ux/Vx: never updated
+          uxo[j * pitch + nx] = uxm_r;
+          if (RECORD) vmx = fmax(vmx, fabs(vxm_r));
+        }
+        if (j == ny - 1) {  // face row ny of Uy/Vy: never updated
+          uyo[ny * pitch + i] = uy0;
+          if (RECORD) vmy = fmax(vmy, fabs(vy0));
+        }
+      }
+      if (RECORD) {
+        vmx = fmax(vmx, fabs(vx));
+        vmy = fmax(vmy, fabs(vy));
+        f.p[q] = pw;
+        f.txx[q] = xw;
+        f.tyy[q] = yw;
+        if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.txy[q] = cw;
+        if (PLASTIC) {
+          f.txyav[q] = tav_o;
+          f.j2[q] = j2_o;
+          if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.j2xy[q] = j2xy_o;
+        }
+      }
+    }
+  }
+}
+
+template <bool PLASTIC, bool RECORD, typename TV>
+__device__ __forceinline__ void stream_segment(const Geo& g, const Fields& f, int src, int strip, int seg, int seg_h,
+                                               StreamWarpSmem<TV>& sm, double& vmx, double& vmy) {
+  const int jA = seg * seg_h;
+  const int jB = min(jA + seg_h, g.ny);
+  if (stream_interior(g.nx, g.ny, strip, jA, jB))
+    stream_task<PLASTIC, RECORD, true, TV>(g, f, src, strip, jA, jB, sm, vmx, vmy);
+  else
+    stream_task<PLASTIC, RECORD, false, TV>(g, f, src, strip, jA, jB, sm, vmx, vmy);
+}
+
+template <bool RECORD>
+__device__ __forceinline__ void stream_fold_vmax(double vmx, double vmy, unsigned long long* vmax) {
+  if (RECORD) {
+    for (int o = 16; o > 0; o >>= 1) {
+      vmx = fmax(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
+      vmy = fmax(vmy, __shfl_xor_sync(0xffffffffu, vmy, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(&vmax[0], (unsigned long long)__double_as_longlong(vmx));
+      atomicMax(&vmax[1], (unsigned long long)__double_as_longlong(vmy));
+    }
+  }
+}
+
+// One RVE: warp w of CTA b handles task b * STREAM_WARPS + w = (strip, segment).
+template <bool PLASTIC, bool RECORD, typename TV>
+__global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream(Geo g, Fields f, int src, int nstrips, int nsegs,
+                                                                   int seg_h) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StreamWarpSmem<TV>& sm = reinterpret_cast<StreamWarpSmem<TV>*>(smem_raw)[threadIdx.x >> 5];
+  const int task = blockIdx.x * STREAM_WARPS + (threadIdx.x >> 5);
+  if (task >= nstrips * nsegs) return;  // whole warp
+  double vmx = 0.0, vmy = 0.0;
+  stream_segment<PLASTIC, RECORD, TV>(g, f, src, task % nstrips, task / nstrips, seg_h, sm, vmx, vmy);
+  stream_fold_vmax<RECORD>(vmx, vmy, f.vmax);
+}
+
+// Many RVEs: a persistent grid of warps walks the device-side list {rve, strip | seg << 16}
+// (warps are independent, so a CTA's warps may work on different RVEs).  `parity` is the
+// launch's position in the captured graph (mod 2), as for the tile form.
+template <bool RECORD, typename TV>
+__global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream_batch(const BatchEntry* __restrict__ ents,
+                                                                         const int2* __restrict__ units,
+                                                                         const int* __restrict__ nunits, int parity,
+                                                                         int seg_h) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StreamWarpSmem<TV>& sm = reinterpret_cast<StreamWarpSmem<TV>*>(smem_raw)[threadIdx.x >> 5];
+  const int n = *nunits;
+  const int nw = gridDim.x * STREAM_WARPS;
+  for (int t = blockIdx.x * STREAM_WARPS + (threadIdx.x >> 5); t < n; t += nw) {
+    const int2 u = units[t];
+    const BatchEntry& e = ents[u.x];
+    const int src = e.src0 ^ parity;
+    double vmx = 0.0, vmy = 0.0;
+    if (e.plastic) stream_segment<true, RECORD, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
+    else stream_segment<false, RECORD, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
+    stream_fold_vmax<RECORD>(vmx, vmy, e.f.vmax);
+  }
+}
+
+}  // namespace ep2d

@@ -1,7 +1,8 @@
-// ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh and
-// ep2d_iter_f64.cuh.
+// ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh,
+// ep2d_iter_f64.cuh (tile form) and ep2d_iter_stream.cuh (stream form).
 #include "ep2d_device.cuh"
 #include "ep2d_iter_f64.cuh"
+#include "ep2d_iter_stream.cuh"
 
 namespace ep2d {
 
@@ -71,9 +72,8 @@ int occupancy_ty(bool record) {
                                                              smem_bytes<TY>());
   return e == cudaSuccess && n > 0 ? n : 1;
 }
-}  // namespace
 
-cudaError_t prepare_kernels() {
+cudaError_t prepare_kernels_impl() {
   cudaError_t e;
   if ((e = set_attrs_ty<8, double>()) != cudaSuccess) return e;
   if ((e = set_attrs_ty<16, double>()) != cudaSuccess) return e;
@@ -83,8 +83,62 @@ cudaError_t prepare_kernels() {
   return set_attrs_ty<32, float>();
 }
 
-cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed, int tile_y,
-                        cudaStream_t stream) {
+template <typename TV>
+cudaError_t launch_stream_tv(const Geo& g, const Fields& f, int src, bool plastic, bool record, int seg_h,
+                             cudaStream_t stream) {
+  const int nstrips = (g.nx + STREAM_COLS - 1) / STREAM_COLS;
+  const int nsegs = (g.ny + seg_h - 1) / seg_h;
+  const int blocks = (nstrips * nsegs + STREAM_WARPS - 1) / STREAM_WARPS;
+  const int threads = 32 * STREAM_WARPS;
+  const size_t sm = stream_smem_bytes<TV>();
+  if (plastic) {
+    if (record) k_iter_stream<true, true, TV><<<blocks, threads, sm, stream>>>(g, f, src, nstrips, nsegs, seg_h);
+    else k_iter_stream<true, false, TV><<<blocks, threads, sm, stream>>>(g, f, src, nstrips, nsegs, seg_h);
+  } else {
+    if (record) k_iter_stream<false, true, TV><<<blocks, threads, sm, stream>>>(g, f, src, nstrips, nsegs, seg_h);
+    else k_iter_stream<false, false, TV><<<blocks, threads, sm, stream>>>(g, f, src, nstrips, nsegs, seg_h);
+  }
+  return cudaGetLastError();
+}
+
+template <typename TV>
+cudaError_t launch_stream_batch_tv(const BatchEntry* ents, const int2* units, const int* nunits, int parity,
+                                   bool record, int seg_h, int blocks, cudaStream_t stream) {
+  const int threads = 32 * STREAM_WARPS;
+  const size_t sm = stream_smem_bytes<TV>();
+  if (record) k_iter_stream_batch<true, TV><<<blocks, threads, sm, stream>>>(ents, units, nunits, parity, seg_h);
+  else k_iter_stream_batch<false, TV><<<blocks, threads, sm, stream>>>(ents, units, nunits, parity, seg_h);
+  return cudaGetLastError();
+}
+
+template <typename TV>
+int stream_occupancy(bool record) {
+  int n = 0;
+  const cudaError_t e =
+      record ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_stream_batch<true, TV>, 32 * STREAM_WARPS,
+                                                             stream_smem_bytes<TV>())
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_stream_batch<false, TV>, 32 * STREAM_WARPS,
+                                                             stream_smem_bytes<TV>());
+  return e == cudaSuccess && n > 0 ? n : 1;
+}
+}  // namespace
+
+cudaError_t prepare_kernels() { return prepare_kernels_impl(); }
+
+void shape_units(const IterShape& s, int nx, int ny, int* ux, int* uy) {
+  const int cols = s.form == FORM_TILE ? TILE_X : STREAM_COLS;
+  *ux = (nx + cols - 1) / cols;
+  *uy = (ny + s.rows - 1) / s.rows;
+}
+
+cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed,
+                        const IterShape& shape, cudaStream_t stream) {
+  if (shape.form == FORM_STREAM) {
+    if (shape.rows < SEG_MIN || shape.rows > SEG_MAX) return cudaErrorInvalidValue;
+    return mixed ? launch_stream_tv<float>(g, f, src, plastic, record, shape.rows, stream)
+                 : launch_stream_tv<double>(g, f, src, plastic, record, shape.rows, stream);
+  }
+  const int tile_y = shape.rows;
   if (mixed) {
     if (tile_y == 8) return launch_iter_ty<8, float>(g, f, src, plastic, record, stream);
     if (tile_y == 32) return launch_iter_ty<32, float>(g, f, src, plastic, record, stream);
@@ -95,19 +149,27 @@ cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bo
   return launch_iter_ty<16, double>(g, f, src, plastic, record, stream);
 }
 
-cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* tiles, const int* ntiles, int parity, bool record,
-                              bool mixed, int tile_y, int blocks, cudaStream_t stream) {
-  if (mixed) {
-    if (tile_y == 8) return launch_batch_ty<8, float>(ents, tiles, ntiles, parity, record, blocks, stream);
-    if (tile_y == 32) return launch_batch_ty<32, float>(ents, tiles, ntiles, parity, record, blocks, stream);
-    return launch_batch_ty<16, float>(ents, tiles, ntiles, parity, record, blocks, stream);
+cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* units, const int* nunits, int parity, bool record,
+                              bool mixed, const IterShape& shape, int blocks, cudaStream_t stream) {
+  if (shape.form == FORM_STREAM) {
+    if (shape.rows < SEG_MIN || shape.rows > SEG_MAX) return cudaErrorInvalidValue;
+    return mixed ? launch_stream_batch_tv<float>(ents, units, nunits, parity, record, shape.rows, blocks, stream)
+                 : launch_stream_batch_tv<double>(ents, units, nunits, parity, record, shape.rows, blocks, stream);
   }
-  if (tile_y == 8) return launch_batch_ty<8, double>(ents, tiles, ntiles, parity, record, blocks, stream);
-  if (tile_y == 32) return launch_batch_ty<32, double>(ents, tiles, ntiles, parity, record, blocks, stream);
-  return launch_batch_ty<16, double>(ents, tiles, ntiles, parity, record, blocks, stream);
+  const int tile_y = shape.rows;
+  if (mixed) {
+    if (tile_y == 8) return launch_batch_ty<8, float>(ents, units, nunits, parity, record, blocks, stream);
+    if (tile_y == 32) return launch_batch_ty<32, float>(ents, units, nunits, parity, record, blocks, stream);
+    return launch_batch_ty<16, float>(ents, units, nunits, parity, record, blocks, stream);
+  }
+  if (tile_y == 8) return launch_batch_ty<8, double>(ents, units, nunits, parity, record, blocks, stream);
+  if (tile_y == 32) return launch_batch_ty<32, double>(ents, units, nunits, parity, record, blocks, stream);
+  return launch_batch_ty<16, double>(ents, units, nunits, parity, record, blocks, stream);
 }
 
-int iter_blocks_per_sm(bool record, bool mixed, int tile_y) {
+int iter_blocks_per_sm(bool record, bool mixed, const IterShape& shape) {
+  if (shape.form == FORM_STREAM) return mixed ? stream_occupancy<float>(record) : stream_occupancy<double>(record);
+  const int tile_y = shape.rows;
   if (mixed) {
     if (tile_y == 8) return occupancy_ty<8, float>(record);
     if (tile_y == 32) return occupancy_ty<32, float>(record);

@@ -63,6 +63,8 @@ int row_pitch(int nx) { return ((nx + 1 + 31) / 32) * 32; }
 int validate_params(const ep2d_params& p) {
   if (p.nx < 8 || p.ny < 8) return fail(EP2D_ERR_ARG, "grid must be at least 8 x 8");
   if (p.nx > (1 << 16) || p.ny > (1 << 16)) return fail(EP2D_ERR_ARG, "grid larger than 65536 per side");
+  if ((int64_t)row_pitch(p.nx) * (p.ny + 1) >= ((int64_t)1 << 31))
+    return fail(EP2D_ERR_ARG, "grid too large: a field would exceed 2^31 elements");
   if (p.nl < 1 || p.nl > EP2D_MAX_NL) return fail(EP2D_ERR_ARG, "nl (NL) must be 1, 2 or 3");
   if (p.check_every < 1) return fail(EP2D_ERR_ARG, "check_every must be >= 1");
   if (p.niter < 0) return fail(EP2D_ERR_ARG, "niter must be >= 0");
@@ -74,7 +76,17 @@ int validate_params(const ep2d_params& p) {
   if (!(p.pa[5] > 0.0)) return fail(EP2D_ERR_ARG, "rho0 must be positive");
   if (!(p.pa[10] >= 1.0) || p.pa[10] > 64.0) return fail(EP2D_ERR_ARG, "N (pores per side) must be in [1, 64]");
   if (!(p.pa[9] >= 0.0)) return fail(EP2D_ERR_ARG, "rad must be >= 0");
+  if (p.kernel < EP2D_KERNEL_AUTO || p.kernel > EP2D_KERNEL_STREAM) return fail(EP2D_ERR_ARG, "unknown kernel form");
+  if (p.rows != 0 && !shape_valid(shape_of(p)))
+    return fail(EP2D_ERR_ARG, "rows must be 8, 16 or 32 for the tile form and 16..1024 for the stream form");
   return EP2D_OK;
+}
+
+IterShape shape_of(const ep2d_params& p) {
+  IterShape s;
+  s.form = p.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
+  s.rows = p.rows ? p.rows : (s.form == FORM_TILE ? TILE_Y : SEG_DEFAULT);
+  return s;
 }
 
 bool host_in_pore(const Derived& d, long nX, long nY, double x, double y) {
@@ -330,6 +342,7 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EP2D_ERR_NODEV, "no CUDA device");
   if (p.device < 0 || p.device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");
   prm = p;
+  shape = shape_of(p);
   device = p.device;
   DeviceScope ds(device);
   rc = prepare_device(device);
@@ -442,7 +455,7 @@ int Rve::reset() {
 }
 
 int Rve::launch_one(bool record) {
-  EP2D_CK(launch_iter(g, f, cur, prm.nl > 1, record, mixed(), tile_y, stream));
+  EP2D_CK(launch_iter(g, f, cur, prm.nl > 1, record, mixed(), shape, stream));
   cur ^= 1;
   return EP2D_OK;
 }
@@ -454,7 +467,7 @@ int Rve::capture(int parity) {
   cur = parity;
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < kGraphLen && le == cudaSuccess; k++) {
-    le = launch_iter(g, f, cur, prm.nl > 1, false, mixed(), tile_y, stream);
+    le = launch_iter(g, f, cur, prm.nl > 1, false, mixed(), shape, stream);
     cur ^= 1;
   }
   cur = saved;

@@ -52,6 +52,9 @@ void final_moduli(int nl, const ep2d_step_record& r0, const ep2d_step_record* r1
 
 // Validate an ep2d_params; returns EP2D_OK or an error status (with message).
 int validate_params(const ep2d_params& p);
+// The iteration kernel a handle uses: the form and rows the parameters name, or the
+// library's choice (the stream form, SEG_DEFAULT rows) where they are 0.
+IterShape shape_of(const ep2d_params& p);
 
 // Device row pitch (elements) for an nx-wide grid.
 int row_pitch(int nx);
@@ -107,7 +110,7 @@ class Rve {
   Derived d{};
   Geo g{};
   Fields f{};
-  int tile_y = TILE_Y;  // tile height of the iteration kernel
+  IterShape shape{};  // form and rows of the iteration kernel (shape_of(prm))
   bool mixed() const { return prm.precision == EP2D_MIXED; }
   int cur = 0;
   int device = 0;

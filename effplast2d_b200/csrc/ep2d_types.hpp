@@ -47,6 +47,25 @@ constexpr int TILE_X = 32;
 constexpr int TILE_Y = 16;
 constexpr int TILE_Y_CHOICES[3] = {8, 16, 32};
 
+// The two forms of the fused iteration kernel: FORM_TILE (CTA per tile, halos in shared
+// memory; rows = tile height) and FORM_STREAM (warp per 28-column strip segment; rows =
+// segment height, SEG_MIN..SEG_MAX).
+enum IterForm { FORM_TILE = 0, FORM_STREAM = 1 };
+constexpr int SEG_MIN = 16, SEG_MAX = 1024;
+constexpr int SEG_DEFAULT = 64;
+constexpr int SEG_CHOICES[3] = {32, 64, 128};
+struct IterShape {
+  int form = FORM_STREAM;
+  int rows = SEG_DEFAULT;
+};
+// true if `s` names a launchable kernel
+inline bool shape_valid(const IterShape& s) {
+  if (s.form == FORM_TILE) return s.rows == 8 || s.rows == 16 || s.rows == 32;
+  return s.form == FORM_STREAM && s.rows >= SEG_MIN && s.rows <= SEG_MAX;
+}
+// work units of one RVE: tiles or strip segments, as (x, y) counts
+void shape_units(const IterShape& s, int nx, int ny, int* ux, int* uy);
+
 // Number of sums produced by the averaging and boundary reductions.
 constexpr int NAVG = 11;
 
@@ -56,13 +75,14 @@ cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream);
 cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
                            int zero_first, cudaStream_t stream);
 // one iteration of one RVE; mixed: velocities stored as float
-cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed, int tile_y,
-                        cudaStream_t stream);
-// one iteration of every RVE in the tile list (persistent grid of `blocks` CTAs)
-cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* tiles, const int* ntiles, int parity, bool record,
-                              bool mixed, int tile_y, int blocks, cudaStream_t stream);
-// CTAs of one tile height resident per SM (occupancy of the batched kernel)
-int iter_blocks_per_sm(bool record, bool mixed, int tile_y);
+cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed,
+                        const IterShape& shape, cudaStream_t stream);
+// one iteration of every RVE in the work list {rve, x | y << 16} (tiles or strip
+// segments of `shape`), by a persistent grid of `blocks` CTAs
+cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* units, const int* nunits, int parity, bool record,
+                              bool mixed, const IterShape& shape, int blocks, cudaStream_t stream);
+// CTAs of the batched kernel of `shape` resident per SM
+int iter_blocks_per_sm(bool record, bool mixed, const IterShape& shape);
 // averaging: writes NAVG sums to `sums` (device); `partials` holds avg_partials_len(g) doubles
 size_t avg_partials_len(const Geo& g);
 cudaError_t launch_average(const Geo& g, const Fields& f, int src, double nu0, int perOffsetX, int perOffsetY,

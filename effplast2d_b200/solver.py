@@ -112,10 +112,11 @@ class Solver:
     """One RVE on the GPU (an ep2d_handle): the reference's EffPlast2D object."""
 
     def __init__(self, nx, ny, pa, nl=1, niter=100000, eiter=1e-9, check_every=10000, device=0,
-                 precision=_abi.FP64):
+                 precision=_abi.FP64, kernel=_abi.KERNEL_AUTO, rows=0):
         self.nx, self.ny = int(nx), int(ny)
         self.params = _abi.make_params(nx, ny, pa, nl=nl, niter=niter, eiter=eiter,
-                                       check_every=check_every, precision=precision, device=device)
+                                       check_every=check_every, precision=precision, device=device,
+                                       kernel=kernel, rows=rows)
         h = ctypes.c_void_p()
         _check(lib().ep2d_create(ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h

@@ -48,6 +48,17 @@ enum {
                             stencil arithmetic, residual, averages and moduli in FP64 */
 };
 
+/* form of the fused iteration kernel (both compute the same iteration, operation for
+ * operation; they differ in how threads map onto the grid) */
+enum {
+  EP2D_KERNEL_AUTO = 0,   /* the library's choice (the stream form; batches: timed) */
+  EP2D_KERNEL_TILE = 1,   /* one CTA per 32-column x `rows`-row tile, stencil halos in
+                             shared memory; rows 8, 16 or 32 */
+  EP2D_KERNEL_STREAM = 2  /* one warp per 28-column strip segment of `rows` rows, marching
+                             up its rows with a register window; neighbours by warp
+                             shuffles; rows 16 to 1024 */
+};
+
 /* pa.dat layout (get_sigma_2D.m:32, read at EffPlast2D.cu:700-707, used at :1563-1573) */
 enum {
   EP2D_PA_DX = 0, EP2D_PA_DY = 1, EP2D_PA_DT = 2, EP2D_PA_K0 = 3, EP2D_PA_G0 = 4,
@@ -84,6 +95,8 @@ typedef struct ep2d_params {
   double eiter;            /* EITER */
   int32_t precision;       /* EP2D_FP64 or EP2D_MIXED */
   int32_t device;          /* DEVICE_IDX */
+  int32_t kernel;          /* EP2D_KERNEL_*; 0 = library's choice (no reference counterpart) */
+  int32_t rows;            /* rows per tile / strip segment; 0 = library's choice */
 } ep2d_params;
 
 /* One time step of one load step: the per-step quantities the reference keeps in
@@ -149,9 +162,11 @@ typedef struct ep2d_batch_config {
   int32_t check_every;    /* output_step */
   int32_t precision;      /* EP2D_FP64 or EP2D_MIXED (FP32 velocity storage) */
   int32_t device;
-  int32_t tile_y;         /* 8, 16 or 32 rows per tile; 0 = pick by timing the first launches */
+  int32_t rows;           /* rows per tile (tile form: 8, 16, 32) or strip segment (stream
+                             form: 16..1024); 0 = pick form and rows by timing the first
+                             launches of the batch */
   int32_t graph_len;      /* iterations per captured CUDA graph (even; 0 = 64) */
-  int32_t reserved;
+  int32_t kernel;         /* EP2D_KERNEL_*; with rows != 0, AUTO means the stream form */
 } ep2d_batch_config;
 
 typedef struct ep2d_batch_stats {
@@ -160,9 +175,12 @@ typedef struct ep2d_batch_stats {
   int64_t launches;       /* batched iteration launches */
   int64_t all_launches;   /* every kernel launched, post-processing included */
   int64_t cell_updates;   /* sum over RVEs of nx*ny per iteration */
-  int32_t tile_y;         /* tile height used */
-  int32_t blocks;         /* persistent grid size */
-  double tune_us[3];      /* measured us per launch for tile heights 8, 16, 32 (0 if untimed) */
+  int32_t rows;           /* rows per tile / strip segment used */
+  int32_t blocks;         /* persistent grid size (CTAs) */
+  int32_t kernel;         /* EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM: the form used */
+  int32_t n_tuned;        /* candidates timed by the autotuner */
+  double tune_us[6];      /* measured us per launch: tile form rows 8, 16, 32, stream form
+                             rows 32, 64, 128 (0 if untimed) */
 } ep2d_batch_stats;
 
 /* ---- library ---------------------------------------------------------------- */

@@ -91,11 +91,15 @@ def test_solver_without_device_fails_loudly():
     assert e.value.status == _abi.ERR_NODEV
 
 
-@pytest.mark.parametrize("bad", ["nan_dx", "nl4", "tiny", "zero_pores"])
+@pytest.mark.parametrize("bad", ["nan_dx", "nl4", "tiny", "zero_pores", "kernel3", "tile_rows12", "stream_rows8",
+                                 "stream_rows2048"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
     pa = ep.make_pa(20.0, 20.0, 32, 32)
     nx, nl = 32, 1
+    kw = {"kernel3": dict(kernel=3), "tile_rows12": dict(kernel=ep.KERNEL_TILE, rows=12),
+          "stream_rows8": dict(kernel=ep.KERNEL_STREAM, rows=8),
+          "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048)}.get(bad, {})
     if bad == "nan_dx":
         pa[0] = float("nan")
     elif bad == "nl4":
@@ -105,7 +109,7 @@ def test_invalid_params_rejected_before_device(bad):
     elif bad == "zero_pores":
         pa[10] = 0.0
     with pytest.raises(ep.EP2DError) as e:
-        ep.Solver(nx, nx, pa, nl=nl)
+        ep.Solver(nx, nx, pa, nl=nl, **kw)
     assert e.value.status == _abi.ERR_ARG
 
 
@@ -121,5 +125,5 @@ def test_batch_and_server_argument_errors():
         B.batch_solve([s], niter=1500, check_every=1000)
     assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)
     with pytest.raises(ep.EP2DError) as e:
-        B.batch_solve([s], niter=2000, check_every=1000, tile_y=12)
+        B.batch_solve([s], niter=2000, check_every=1000, rows=12)
     assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)

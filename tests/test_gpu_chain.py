@@ -77,7 +77,13 @@ def test_eff_moduli_chain(case):
     for kind in ("num", "num_per", "an", "an_per"):
         keys = ["kphi", "kd"] + (["g"] if nl == 3 else [])
         for k in keys:
-            assert close(rg[kind][k], ro[kind][k], 1e-8), (kind, k, rg[kind][k], ro[kind][k])
+            a, b = rg[kind][k], ro[kind][k]
+            if not math.isfinite(b):
+                # a load type with equal xx and yy parts leaves G's denominator exactly
+                # zero; the quotient is +-inf or nan by the sign of rounding noise
+                assert not math.isfinite(a), (kind, k, a, b)
+                continue
+            assert close(a, b, 1e-8), (kind, k, a, b)
     assert rg["total_iterations"] == ro["total_iterations"]
     # final fields
     for f in ("P", "tauXX", "tauYY", "tauXY", "Ux", "Uy"):

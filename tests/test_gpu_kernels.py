@@ -4,8 +4,11 @@ Both sides start from the same seeded state and run the same number of iteration
 the reference's sequence ComputeStress -> [ComputeJ2 -> ComputePlasticity] ->
 ComputeDisp (EffPlast2D.cu:389-399).  The GPU contracts multiply-adds (as the
 reference's own CUDA build does); the oracle does not.  Tolerance: every field within
-1e-11 of its max-abs after one iteration and 1e-9 after hundreds (north-star bar for
-fields: 1e-6).
+1e-11 of its max-abs after one iteration and 1e-9 after hundreds (bar for fields:
+1e-6).  Both kernel forms are checked: the tile form (CTA per tile, halos in shared
+memory) and the stream form (warp per strip segment, neighbours by shuffles), the
+latter with segments of 16 rows too, so that grids hold several segments, a ragged
+last segment and a ragged last strip.
 """
 import numpy as np
 import pytest
@@ -17,6 +20,8 @@ pytestmark = pytest.mark.gpu
 
 FIELDS = ["P", "tauXX", "tauYY", "tauXY", "Ux", "Uy", "Vx", "Vy"]
 PLASTIC_FIELDS = ["tauXYav", "J2", "J2XY"]
+FORMS = [(ep.KERNEL_TILE, 16), (ep.KERNEL_STREAM, 16), (ep.KERNEL_STREAM, 64)]
+FORM_IDS = ["tile16", "stream16", "stream64"]
 
 
 def _pa(n_x, n_y, n_pores=1, porosity=0.01, yield_stress=1.0, g0=0.5):
@@ -43,8 +48,8 @@ def _random_state(nx, ny, seed, strain=6e-5, noise=2e-6, vnoise=1e-7):
     return {"Ux": ux, "Uy": uy, "Vx": vx, "Vy": vy}
 
 
-def _pair(nx, ny, pa, nl):
-    return ep.Solver(nx, ny, pa, nl=nl), oracle.Oracle(nx, ny, pa, nl=nl)
+def _pair(nx, ny, pa, nl, form=(ep.KERNEL_AUTO, 0)):
+    return ep.Solver(nx, ny, pa, nl=nl, kernel=form[0], rows=form[1]), oracle.Oracle(nx, ny, pa, nl=nl)
 
 
 @pytest.mark.parametrize("nx,ny,n_pores", [(64, 64, 1), (96, 96, 3), (64, 96, 2), (40, 56, 1), (129, 71, 2)])
@@ -65,12 +70,13 @@ def test_materials_and_masks(nx, ny, n_pores):
     assert np.array_equal(g.get("tauXY") == 0.0, corner.astype(bool))
 
 
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("nl", [1, 2, 3])
 @pytest.mark.parametrize("nx,ny,n_pores", [(64, 64, 1), (96, 64, 3), (40, 56, 2), (33, 65, 1)])
-def test_one_iteration_random_state(nl, nx, ny, n_pores, rel):
+def test_one_iteration_random_state(nl, nx, ny, n_pores, form, rel):
     # Y small enough that a good part of the grid yields
     pa = _pa(nx, ny, n_pores=n_pores, porosity=0.02, yield_stress=2e-5)
-    g, o = _pair(nx, ny, pa, nl)
+    g, o = _pair(nx, ny, pa, nl, form)
     st = _random_state(nx, ny, 7 + nl)
     for k, v in st.items():
         g.set(k, v)
@@ -85,11 +91,12 @@ def test_one_iteration_random_state(nl, nx, ny, n_pores, rel):
         assert (j2 > pa[8]).mean() > 0.05  # the return map is exercised
 
 
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("nl", [1, 3])
-def test_many_iterations(nl, rel):
+def test_many_iterations(nl, form, rel):
     nx = ny = 96
     pa = _pa(nx, ny, n_pores=3, porosity=0.02, yield_stress=1e-5)
-    g, o = _pair(nx, ny, pa, nl)
+    g, o = _pair(nx, ny, pa, nl, form)
     st = _random_state(nx, ny, 3, noise=0.0, vnoise=0.0)
     for k, v in st.items():
         g.set(k, v)
@@ -122,3 +129,24 @@ def test_homogeneous_affine_is_equilibrium():
     assert np.max(np.abs(g.get("Vx"))) < 1e-16  # rounding of the affine differences only
     P = g.get("P")
     assert np.allclose(P, P[1, 1], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("rows", [16, 64, 256])
+def test_stream_form_matches_tile_form(rows):
+    # Both forms evaluate the same explicitly rounded per-cell formulas, so they agree
+    # bit for bit.  The grid is wider and taller than several strips and segments,
+    # ragged in both, so interior and edge segments both run.
+    nx, ny = 301, 203
+    pa = _pa(nx, ny, n_pores=4, porosity=0.03, yield_stress=1e-5)
+    st = _random_state(nx, ny, 11)
+    out = []
+    for kernel, r in ((ep.KERNEL_TILE, 16), (ep.KERNEL_STREAM, rows)):
+        g = ep.Solver(nx, ny, pa, nl=3, kernel=kernel, rows=r)
+        for k, v in st.items():
+            g.set(k, v)
+        g.iterate(1)
+        g.iterate(300)
+        out.append({f: g.get(f) for f in FIELDS + PLASTIC_FIELDS})
+    for f in FIELDS + PLASTIC_FIELDS:
+        assert np.array_equal(out[1][f], out[0][f]), (f, float(np.max(np.abs(out[1][f] - out[0][f]))))
+
