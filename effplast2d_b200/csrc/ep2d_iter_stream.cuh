@@ -31,8 +31,10 @@ namespace ep2d {
 
 constexpr int STREAM_COLS = 28;                 // owned columns per warp
 constexpr int STREAM_WARPS = 4;                 // warps per CTA
-constexpr int STREAM_DEPTH = 8;                 // rows of loads in flight per warp
-constexpr int STREAM_SLOTS = STREAM_DEPTH + 1;  // the slot refilled was read one step earlier
+constexpr int STREAM_DEPTH = 6;                 // rows of loads in flight per warp
+// rows k-2 .. k+DEPTH live in the ring at step k: the faces of row k-2 read U and V of
+// rows k-2 and k-1 from it, and the refill goes to the slot of row k-3
+constexpr int STREAM_SLOTS = STREAM_DEPTH + 3;
 
 // One row of a warp's 32 columns, as the ring holds it; m: the aligned 32-bit word of
 // the byte mask that contains the lane's node.
@@ -45,12 +47,13 @@ struct StreamRow {
   uint32_t m[32];
 };
 
-// Shared memory of one warp: its ring, then the 16-entry table of corner_g4 by the
-// material bits of the four nodes around a corner.
+// Shared memory of one warp: its ring, the 16-entry table of corner_g4 by the material
+// bits of the four nodes around a corner, and (K, 2G) by the material bit of a node.
 template <typename TV>
 struct StreamWarpSmem {
   StreamRow<TV> ring[STREAM_SLOTS];
   double g4[16];
+  double2 kg[2];
 };
 
 template <typename TV>
@@ -104,6 +107,8 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   const bool colx = INTERIOR || (i >= 0 && i <= nx);  // column of Ux / Vx
   const bool coln = INTERIOR || (i >= 0 && i < nx);   // column of nodes, Uy, Vy
   const int mshift = 8 * (i & 3);                     // pitch % 32 == 0: byte i & 3 of the word
+  const int ln1 = min(lane + 1, 31);                  // the lane of column i + 1 (lane 31: unused)
+  const int mshift1 = 8 * ((i + 1) & 3);
 
   // rows k_first .. k_last pass through the ring: U and the mask are needed up to row
   // r + 1 and V up to row r for steps r = jA - 2 .. jB
@@ -120,30 +125,28 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     cp_async_zfill<(int)sizeof(TV)>(&row.vy[lane], fvy + (ry ? q : 0), ry);
     cp_async_zfill<4>(&row.m[lane], mask + (rm ? (q & ~3) : 0), rm);
   };
-  int slot_rd = 0, slot_wr = 0;
+  int slot_wr = 0;
 #pragma unroll 1
   for (int d = 0; d < STREAM_DEPTH; d++) {
     if (k_first + d <= k_last) issue(k_first + d, slot_wr);
     cp_async_commit();  // empty groups keep the count uniform
-    slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
+    slot_wr++;
   }
 
   const double rdX = g.rdX, rdY = g.rdY, third = 1.0 / 3.0;
   const double coh = g.coh, coh2 = g.coh2;
   const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
-  const double K0 = g.K0, Kp = g.Kp, G0 = g.G0, Gp = g.Gp;
-  const double G20 = __dmul_rn(2.0, G0), G2p = __dmul_rn(2.0, Gp);
-  __syncwarp();  // the previous segment of this warp has stopped reading the table
-  if (lane < 16) sm.g4[lane] = corner_g4_of_bits(lane, G0, Gp);
+  __syncwarp();  // the previous segment of this warp has stopped reading the tables
+  if (lane < 16) sm.g4[lane] = corner_g4_of_bits(lane, g.G0, g.Gp);
+  if (lane < 2) sm.kg[lane] = make_double2(lane ? g.Kp : g.K0, __dmul_rn(2.0, lane ? g.Gp : g.G0));
   __syncwarp();
 
-  // windows at step r: U rows r-1 (m), r (0), r+1 (p); masks rows r, r+1; V rows r-1,
-  // r, r+1 (m, 0, n).  Suffix _r: the value of the lane to the right (column i+1),
-  // _l: to the left (column i-1).
-  double uxm = 0.0, ux0 = 0.0, uxp = 0.0, uym = 0.0, uy0 = 0.0, uyp = 0.0;
-  double uxp_r = 0.0;  // Ux(i+1, r+1); at the next step Ux(i+1, r)
-  int mk0 = 0, mkp = 0, mkp_r = 0;
-  double vxm = 0.0, vx0 = 0.0, vxn = 0.0, vym = 0.0, vy0 = 0.0, vyn = 0.0;
+  // registers at step r (suffix _r: column i+1, _l: column i-1): U rows r (0) and r+1
+  // (p), masks rows r and r+1; U and V of row r-1 and r are read back from the ring
+  double ux0 = 0.0, uxp = 0.0, uy0 = 0.0, uyp = 0.0;
+  double ux0_r = 0.0, uxp_r = 0.0;  // Ux(i+1, r), Ux(i+1, r+1)
+  int mk0 = 0, mkp = 0, mk0_r = 0, mkp_r = 0;
+  int g_lo = 0, g_hi = 0;  // material bits of nodes (i, i+1) in rows r and r+1
   // trial stresses: nodes rows r-1 (a) and r (b); corners rows r-3..r (c0..c3)
   double xa = 0.0, ya = 0.0, pb = 0.0, xb = 0.0, yb = 0.0, pa_ = 0.0;
   double xb_r = 0.0, yb_r = 0.0;  // node trial row r of column i+1; next step: row r-1
@@ -153,33 +156,29 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   double pq = 0.0, yq = 0.0, pw = 0.0, xw = 0.0, yw = 0.0, cq = 0.0, cw = 0.0;
   double cw_l = 0.0;  // returned corner row r-1 of column i-1; next step: row r-2
 
-  double ux0_r = 0.0;  // Ux(i+1, r)
-  int mk0_r = 0;
-  int g_lo = 0, g_hi = 0;  // material bits of nodes (i, i+1) in rows r and r+1
+  // slots of rows k, k-1, k-2
+  int s_k = STREAM_SLOTS - 1, s_k1 = STREAM_SLOTS - 2, s_k2 = STREAM_SLOTS - 3;
   int k = k_first;
-  // bring row k from the ring into the windows and refill the ring
+  // bring row k from the ring into the registers and refill the ring
   auto take_row = [&]() {
-    cp_async_wait<STREAM_DEPTH - 1>();  // row k has landed
-    ux0_r = uxp_r;
-    mk0_r = mkp_r;
-    {
-      const StreamRow<TV>& row = sm.ring[slot_rd];
-      uxm = ux0; ux0 = uxp; uxp = row.ux[lane];
-      uym = uy0; uy0 = uyp; uyp = row.uy[lane];
-      mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
-      vxm = vx0; vx0 = vxn; vxn = (double)row.vx[lane];
-      vym = vy0; vy0 = vyn; vyn = (double)row.vy[lane];
-    }
-    slot_rd = (slot_rd + 1 == STREAM_SLOTS) ? 0 : slot_rd + 1;
-    if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr);
-    cp_async_commit();
-    slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
-    uxp_r = shfl_dn(uxp);
-    mkp_r = shfl_dn_i(mkp);
+    cp_async_wait<STREAM_DEPTH - 1>();  // this lane's copies of row k have landed
+    __syncwarp();                        // ... and every lane's (neighbours are read below)
+    s_k2 = s_k1;
+    s_k1 = s_k;
+    s_k = (s_k + 1 == STREAM_SLOTS) ? 0 : s_k + 1;
+    const StreamRow<TV>& row = sm.ring[s_k];
+    ux0 = uxp; uxp = row.ux[lane];
+    ux0_r = uxp_r; uxp_r = row.ux[ln1];
+    uy0 = uyp; uyp = row.uy[lane];
+    mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
+    mk0_r = mkp_r; mkp_r = (int)((row.m[ln1] >> mshift1) & 0xffu);
     g_lo = g_hi;
     g_hi = (mkp & M_MAT) | ((mkp_r & M_MAT) << 1);
+    if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr);  // the slot of row k-3
+    cp_async_commit();
+    slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
   };
-  take_row();  // rows k_first and k_first + 1 only fill the windows
+  take_row();  // rows k_first and k_first + 1 only fill the registers
   k++;
   take_row();
   k++;
@@ -189,11 +188,12 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     const int r = k - 1;
 
     // ---- trial stresses of row r
-    const double uyp_r = shfl_dn(uyp);
+    const double uyp_r = sm.ring[s_k].uy[ln1];
     double pn = 0.0, xn = 0.0, yn = 0.0, cn = 0.0;
-    if ((INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE))
-      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), (mk0 & M_MAT) ? Kp : K0, (mk0 & M_MAT) ? G2p : G20, rdX,
-                 rdY, third, pn, xn, yn);
+    if ((INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE)) {
+      const double2 kg = sm.kg[mk0 & M_MAT];
+      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), kg.x, kg.y, rdX, rdY, third, pn, xn, yn);
+    }
     if ((INTERIOR || (i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1)) && !(mk0 & M_CORNER))
       cn = corner_trial(sm.g4[g_lo | (g_hi << 2)], __dsub_rn(uxp_r, ux0_r), __dsub_rn(uyp_r, uyp), rdX, rdY);
     const double xa_r = xb_r, ya_r = yb_r;
@@ -250,14 +250,12 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     pw = pa_; xw = xr; yw = yr; cw = cr;
     cw_l = shfl_up1(cw);
 
-    // ---- faces of row j (owned rows [jA, jB))
+    // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring
     const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
-    double uxm_r = 0.0, vxm_r = 0.0;
-    if (!INTERIOR) {
-      uxm_r = shfl_dn(uxm);
-      vxm_r = shfl_dn(vxm);
-    }
     if (j >= jA && own) {
+      const StreamRow<TV>& rj = sm.ring[s_k2];
+      const double uxm = rj.ux[lane], uym = rj.uy[lane];
+      const double vxm = (double)rj.vx[lane], vym = (double)rj.vy[lane];
       const int q = j * pitch + i;
       double vx = vxm;
       if (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) {
@@ -276,13 +274,14 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       }
       uyo[q] = advance(uym, vy, dT);
       if (!INTERIOR) {
-        if (i == nx - 1) {  // face column nx of Ux/Vx: never updated
-          uxo[j * pitch + nx] = uxm_r;
-          if (RECORD) vmx = fmax(vmx, fabs(vxm_r));
+        if (i == nx - 1) {  // face column nx of Ux/Vx (lane + 1): never updated
+          uxo[j * pitch + nx] = rj.ux[lane + 1];
+          if (RECORD) vmx = fmax(vmx, fabs((double)rj.vx[lane + 1]));
         }
-        if (j == ny - 1) {  // face row ny of Uy/Vy: never updated
-          uyo[ny * pitch + i] = uy0;
-          if (RECORD) vmy = fmax(vmy, fabs(vy0));
+        if (j == ny - 1) {  // face row ny of Uy/Vy (row k-1 of the ring): never updated
+          const StreamRow<TV>& rj1 = sm.ring[s_k1];
+          uyo[ny * pitch + i] = rj1.uy[lane];
+          if (RECORD) vmy = fmax(vmy, fabs((double)rj1.vy[lane]));
         }
       }
       if (RECORD) {
