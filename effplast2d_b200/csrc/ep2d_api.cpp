@@ -191,6 +191,13 @@ int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t
   return EP2D_OK;
 }
 
+int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  if (kernel) *kernel = h->rve.shape.form == ep2d::FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;
+  if (rows) *rows = h->rve.shape.rows;
+  return EP2D_OK;
+}
+
 // sizeof() of every ABI struct, for the binding's layout check
 int ep2d_abi_sizes(int64_t* out, int32_t n) {
   const int64_t s[7] = {(int64_t)sizeof(ep2d_params),      (int64_t)sizeof(ep2d_step_record),

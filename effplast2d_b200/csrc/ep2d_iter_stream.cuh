@@ -29,8 +29,7 @@
 
 namespace ep2d {
 
-constexpr int STREAM_COLS = 28;                 // owned columns per warp
-constexpr int STREAM_WARPS = 4;                 // warps per CTA
+constexpr int STREAM_WARPS = 4;                 // warps per CTA (STREAM_COLS owned columns per warp)
 constexpr int STREAM_DEPTH = 6;                 // rows of loads in flight per warp
 // rows k-2 .. k+DEPTH live in the ring at step k: the faces of row k-2 read U and V of
 // rows k-2 and k-1 from it, and the refill goes to the slot of row k-3

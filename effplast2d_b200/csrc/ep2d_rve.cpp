@@ -82,10 +82,15 @@ int validate_params(const ep2d_params& p) {
   return EP2D_OK;
 }
 
-IterShape shape_of(const ep2d_params& p) {
+IterShape shape_of(const ep2d_params& p, int sm_count) {
   IterShape s;
   s.form = p.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
   s.rows = p.rows ? p.rows : (s.form == FORM_TILE ? TILE_Y : SEG_DEFAULT);
+  if (p.rows == 0 && s.form == FORM_STREAM && sm_count > 0) {
+    const int64_t strips = (p.nx + STREAM_COLS - 1) / STREAM_COLS;
+    s.rows = 64;
+    while (s.rows > SEG_MIN && strips * ((p.ny + s.rows - 1) / s.rows) < 16 * (int64_t)sm_count) s.rows /= 2;
+  }
   return s;
 }
 
@@ -342,11 +347,13 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EP2D_ERR_NODEV, "no CUDA device");
   if (p.device < 0 || p.device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");
   prm = p;
-  shape = shape_of(p);
   device = p.device;
   DeviceScope ds(device);
   rc = prepare_device(device);
   if (rc) return rc;
+  int sms = 0;
+  EP2D_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  shape = shape_of(p, sms);
   d = derive(p);
   rc = hole_samples(d, p.nx, p.ny, &holes);
   if (rc) return rc;
@@ -510,6 +517,7 @@ int Rve::reset_vmax() {
 int Rve::iterate(int64_t n, bool record_last) {
   if (n <= 0) return EP2D_OK;
   DeviceScope ds(device);
+  EP2D_CK(cudaEventRecord(ev_[0], stream));
   int rc = run_plain(record_last ? n - 1 : n);
   if (rc) return rc;
   if (record_last) {
@@ -519,6 +527,11 @@ int Rve::iterate(int64_t n, bool record_last) {
     if (rc) return rc;
     launches++;
   }
+  EP2D_CK(cudaEventRecord(ev_[1], stream));
+  EP2D_CK(cudaEventSynchronize(ev_[1]));
+  float ms = 0.0f;
+  EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+  kernel_ms += ms;
   cell_updates += n * (int64_t)prm.nx * prm.ny;
   return EP2D_OK;
 }

@@ -51,6 +51,7 @@ constexpr int TILE_Y_CHOICES[3] = {8, 16, 32};
 // memory; rows = tile height) and FORM_STREAM (warp per 28-column strip segment; rows =
 // segment height, SEG_MIN..SEG_MAX).
 enum IterForm { FORM_TILE = 0, FORM_STREAM = 1 };
+constexpr int STREAM_COLS = 28;  // columns a warp of the stream form owns (32 lanes, 2-lane halos)
 constexpr int SEG_MIN = 16, SEG_MAX = 1024;
 constexpr int SEG_DEFAULT = 64;
 constexpr int SEG_CHOICES[3] = {32, 64, 128};

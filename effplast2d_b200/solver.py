@@ -23,7 +23,7 @@ EXPORTS = (
     "ep2d_set_field", "ep2d_solve_step", "ep2d_get_record", "ep2d_get_check_errors",
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
-    "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc",
+    "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc", "ep2d_get_kernel_shape",
 )
 
 
@@ -72,6 +72,7 @@ def lib():
         L.ep2d_server_stats.argtypes = [vp, P(i64), P(i64), P(i64), P(i64), P(_abi.BatchStats)]
         L.ep2d_server_destroy.argtypes = [vp]
         L.ep2d_average_fields_noalloc.argtypes = [i32, i32, P(d)] + [vp] * 8
+        L.ep2d_get_kernel_shape.argtypes = [vp, P(i32), P(i32)]
         _lib = L
     return _lib
 
@@ -211,3 +212,9 @@ class Solver:
                                     ctypes.byref(al)))
         return {"kernel_ms": ms.value, "launches": la.value, "cell_updates": cu.value,
                 "all_launches": al.value}
+
+    def kernel_shape(self):
+        """(kernel form, rows) of the iteration kernel this solver launches"""
+        k, r = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().ep2d_get_kernel_shape(self._h, ctypes.byref(k), ctypes.byref(r)))
+        return k.value, r.value

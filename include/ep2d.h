@@ -215,7 +215,8 @@ int ep2d_reset(ep2d_handle* h);
 /* Exactly n pseudo-time iterations of the reference's kernel sequence
  * ComputeStress -> [ComputeJ2 -> ComputePlasticity if nl > 1] -> ComputeDisp
  * (EffPlast2D.cu:389-399), with no convergence check.  Stress-type fields
- * (P, tau*, J2*) hold the last iteration's values afterwards. */
+ * (P, tau*, J2*) hold the last iteration's values afterwards.  Returns when the
+ * iterations have completed; their device time is added to ep2d_get_stats' kernel_ms. */
 int ep2d_iterate(ep2d_handle* h, int64_t n_iter);
 
 /* SaveMatrix's device->host copy (EffPlast2D.cu:795-799) / the H2D copies of
@@ -322,6 +323,10 @@ int ep2d_abi_sizes(int64_t* out, int32_t n);
  * preload, reductions and gathers).  Any pointer may be NULL. */
 int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* iter_launches, int64_t* cell_updates,
                    int64_t* all_launches);
+/* The iteration kernel this handle launches: EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM and
+ * its rows per tile / strip segment (the parameters' choice, or the library's).  No
+ * counterpart in the reference. */
+int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows);
 
 #ifdef __cplusplus
 }
