@@ -10,6 +10,7 @@ from ctypes import c_double, c_int32, c_int64
 
 NPARS = 11
 MAX_NL = 3
+MAX_STEPS = 64  # load steps of the damping mode (nl >= 4)
 
 OK = 0
 ERR_ARG = 1

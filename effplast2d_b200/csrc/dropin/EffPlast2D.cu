@@ -1,6 +1,7 @@
 // EffPlast2D.cu -- drop-in implementation of the reference's EffPlast2D class on top of
 // the libep2d C ABI.  Control flow, messages and output files follow the reference's
-// EffPlast2D.cu (constructor :1541-1612, ComputeEffModuli :179-229, ComputeEffParams
+// EffPlast2D.cu (constructor :1541-1612, ComputeEffModuli :179-229, ComputeEffDamping
+// :230-310, ComputeEffParams
 // printing :311-698, SaveAnStatic2D output :1060-1292, print* :1295-1409, calc* logging
 // :1412-1454); the numerics run in libep2d on the GPU.
 //
@@ -59,7 +60,7 @@ EffPlast2D::EffPlast2D(const unsigned int nTimeSteps) : nTimeSteps_(nTimeSteps) 
   const double rad = prm_.pa[9];
   Y = prm_.pa[8] / std::sqrt(2.0);
   nPores = prm_.pa[10];
-  if (NL <= 3) Check(ep2d_create(&prm_, &h_), __LINE__);
+  Check(ep2d_create(&prm_, &h_), __LINE__);
   log_file.open("EffPlast2D.log", std::ios_base::app);
   const double lX = (nX - 1) * dX;
   const double lY = (nY - 1) * dY;
@@ -116,9 +117,51 @@ double EffPlast2D::ComputeEffModuli(const double initLoadValue, const std::array
   return 0.0;
 }
 
-double EffPlast2D::ComputeEffDamping(const double, const std::array<double, 3>&, const double) {
+// ComputeEffDamping (EffPlast2D.cu:230-310): the preload, NL-1 sinusoidal increments of
+// loadValue along loadType, the strain and stress tensors of every step on stdout, the
+// static fields.  The reference never assigns loadType_ on this path, so its
+// SaveAnStatic2D there reads an uninitialised array to choose the analytic branch
+// (EffPlast2D.h:81, EffPlast2D.cu:1062-1064); here the load type of the call decides.
+// With nPores > 1 (no analytic fields) the outputs do not depend on that choice.
+double EffPlast2D::ComputeEffDamping(const double initLoadValue, const std::array<double, 3>& loadType,
+                                     const double loadValue) {
   if (NL < 4) throw std::invalid_argument("ERROR:  Wrong number of loads in ComputeEffModuli()!\n");
-  throw std::invalid_argument("ERROR:  the damping calculation (NL >= 4) is not part of this build\n");
+  const auto start = std::chrono::system_clock::now();
+  printCalculationType();
+  int64_t total = 0;
+  Check(ep2d_compute_eff_damping(h_, initLoadValue, loadType.data(), static_cast<int32_t>(nTimeSteps_), loadValue,
+                                 &total),
+        __LINE__);
+  ComputeEffParams(0, nTimeSteps_);
+  for (size_t i = 1; i < NL; i++) ComputeEffParams(i, 1);
+  // the record of step i's tensor: (0, nTimeSteps-1) for the preload, (i, 0) after it
+  auto rec = [this](size_t i) {
+    ep2d_step_record r{};
+    Check(ep2d_get_record(h_, static_cast<int32_t>(i), i == 0 ? static_cast<int32_t>(nTimeSteps_) - 1 : 0, &r),
+          __LINE__);
+    return r;
+  };
+  auto table = [&](const char* title, int n, auto get) {
+    std::cout << title;
+    for (size_t i = 0; i < NL; i++) {
+      std::cout << i << ") ";
+      const ep2d_step_record r = rec(i);
+      for (int j = 0; j < n; j++) std::cout << get(r)[j] << " ";
+      std::cout << "\n";
+    }
+  };
+  table("\nStrain tensors:\n", 3, [](const ep2d_step_record& r) { return r.macro_strain; });
+  table("\nStrain tensors periodic:\n", 3, [](const ep2d_step_record& r) { return r.eps_per; });
+  table("\nStress tensors:\n", 4, [](const ep2d_step_record& r) { return r.sigma; });
+  table("\nStress tensors periodic:\n", 4, [](const ep2d_step_record& r) { return r.sigma_per; });
+  if (nTimeSteps_ > 0) {
+    const ep2d_step_record r0 = rec(0);
+    SaveAnStatic2D(r0.delta_p, r0.tau_infty);
+  }
+  const auto end = std::chrono::system_clock::now();
+  const int elapsed_sec = static_cast<int>(std::chrono::duration_cast<std::chrono::seconds>(end - start).count());
+  printDuration(elapsed_sec);
+  return 0.0;
 }
 
 // The printing of ComputeEffParams (EffPlast2D.cu:311-698) from the step's records.

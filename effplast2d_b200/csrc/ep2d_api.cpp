@@ -145,7 +145,7 @@ int ep2d_solve_step(ep2d_handle* h, int32_t step, double load_step_value, const 
 
 int ep2d_get_record(ep2d_handle* h, int32_t step, int32_t time_step, ep2d_step_record* out) {
   if (!h || !out) return fail(EP2D_ERR_ARG, "null argument");
-  if (step < 0 || step >= EP2D_MAX_NL || time_step < 0 || time_step >= h->rve.nts[step])
+  if (step < 0 || step >= (int)h->rve.nts.size() || time_step < 0 || time_step >= h->rve.nts[step])
     return fail(EP2D_ERR_ARG, "no record for this (step, time_step)");
   *out = h->rve.rec[step][time_step];
   return EP2D_OK;
@@ -154,7 +154,7 @@ int ep2d_get_record(ep2d_handle* h, int32_t step, int32_t time_step, ep2d_step_r
 int ep2d_get_check_errors(ep2d_handle* h, int32_t step, int32_t time_step, double* errors_out, int32_t max_n,
                           int32_t* n_out) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
-  if (step < 0 || step >= EP2D_MAX_NL || time_step < 0 || time_step >= h->rve.nts[step])
+  if (step < 0 || step >= (int)h->rve.nts.size() || time_step < 0 || time_step >= h->rve.nts[step])
     return fail(EP2D_ERR_ARG, "no record for this (step, time_step)");
   const std::vector<double>& c = h->rve.checks[step][time_step];
   if (n_out) *n_out = (int32_t)c.size();
@@ -166,6 +166,14 @@ int ep2d_compute_eff_moduli(ep2d_handle* h, double init_load_value, const double
                             int32_t n_time_steps, ep2d_result* out) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
   EP2D_GUARD({ return h->rve.compute_eff_moduli(init_load_value, load_type, n_time_steps, out); })
+}
+
+int ep2d_compute_eff_damping(ep2d_handle* h, double init_load_value, const double load_type[3],
+                             int32_t n_time_steps, double load_value, int64_t* total_iterations) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  EP2D_GUARD({
+    return h->rve.compute_eff_damping(init_load_value, load_type, n_time_steps, load_value, total_iterations);
+  })
 }
 
 int ep2d_static_fields(ep2d_handle* h, double* unu_abs, double* j1nu, double* j2nu) {

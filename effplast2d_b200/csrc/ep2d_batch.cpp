@@ -155,6 +155,8 @@ int BatchEngine::begin_task_step(Slot& s) {
 int BatchEngine::add(const ep2d_rve_spec& spec, uint64_t ticket, double submit_s, int* slot_out) {
   DeviceScope ds(device);
   if (spec.n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
+  if (spec.nl < 1 || spec.nl > EP2D_MAX_NL)
+    return fail(EP2D_ERR_ARG, "a batch runs ComputeEffModuli: nl must be 1, 2 or 3");
   int slot = -1;
   for (size_t k = 0; k < slots_.size(); k++)
     if (!slots_[k].used) {

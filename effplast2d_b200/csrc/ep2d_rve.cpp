@@ -65,7 +65,7 @@ int validate_params(const ep2d_params& p) {
   if (p.nx > (1 << 16) || p.ny > (1 << 16)) return fail(EP2D_ERR_ARG, "grid larger than 65536 per side");
   if ((int64_t)row_pitch(p.nx) * (p.ny + 1) >= ((int64_t)1 << 31))
     return fail(EP2D_ERR_ARG, "grid too large: a field would exceed 2^31 elements");
-  if (p.nl < 1 || p.nl > EP2D_MAX_NL) return fail(EP2D_ERR_ARG, "nl (NL) must be 1, 2 or 3");
+  if (p.nl < 1 || p.nl > EP2D_MAX_STEPS) return fail(EP2D_ERR_ARG, "nl (NL) must be in [1, 64]");
   if (p.check_every < 1) return fail(EP2D_ERR_ARG, "check_every must be >= 1");
   if (p.niter < 0) return fail(EP2D_ERR_ARG, "niter must be >= 0");
   if (p.precision != EP2D_FP64 && p.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
@@ -438,6 +438,9 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   EP2D_CK(cudaEventCreate(&ev_[1]));
   EP2D_CK(cudaStreamSynchronize(stream));
   cur = 0;
+  nts.assign(prm.nl, 0);
+  rec.assign(prm.nl, {});
+  checks.assign(prm.nl, {});
   return EP2D_OK;
 }
 
@@ -449,11 +452,9 @@ int Rve::reset() {
   EP2D_CK(cudaMemsetAsync(dmem, 0, bytes, stream));
   EP2D_CK(cudaStreamSynchronize(stream));
   cur = 0;
-  for (int s = 0; s < EP2D_MAX_NL; s++) {
-    nts[s] = 0;
-    rec[s].clear();
-    checks[s].clear();
-  }
+  nts.assign(prm.nl, 0);
+  rec.assign(prm.nl, {});
+  checks.assign(prm.nl, {});
   ces[0] = ces[1] = ces[2] = 0.0;
   load_type_[0] = load_type_[1] = load_type_[2] = 0.0;
   have_step0 = false;
@@ -702,6 +703,8 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
 int Rve::compute_eff_moduli(double init, const double lt[3], int n_time_steps, ep2d_result* out) {
   if (!lt) return fail(EP2D_ERR_ARG, "load_type is null");
   if (n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
+  // EffPlast2D.cu:182-184
+  if (prm.nl > EP2D_MAX_NL) return fail(EP2D_ERR_ARG, "Wrong number of loads in ComputeEffModuli(): nl > 3");
   begin_chain(lt);
   for (int step = 0; step < prm.nl; step++) {
     double lsv, lts[3];
@@ -711,6 +714,34 @@ int Rve::compute_eff_moduli(double init, const double lt[3], int n_time_steps, e
     if (rc) return rc;
   }
   finish_chain(n_time_steps, out);
+  return EP2D_OK;
+}
+
+// The increments of ComputeEffDamping (EffPlast2D.cu:240-243): load_value times the
+// difference of sin(i 2 pi' / (NL-1)) between consecutive steps, pi' = 3.1415926.
+double Rve::damping_step_value(int step, int nl, double load_value) {
+  return load_value * (std::sin(step * 2.0 * 3.1415926 / (nl - 1)) - std::sin((step - 1) * 2.0 * 3.1415926 / (nl - 1)));
+}
+
+int Rve::compute_eff_damping(double init, const double lt[3], int n_time_steps, double load_value,
+                             int64_t* total_iterations) {
+  if (!lt) return fail(EP2D_ERR_ARG, "load_type is null");
+  if (n_time_steps < 1) return fail(EP2D_ERR_ARG, "n_time_steps must be >= 1");
+  // EffPlast2D.cu:233-235
+  if (prm.nl < 4) return fail(EP2D_ERR_ARG, "Wrong number of loads in ComputeEffDamping(): nl < 4");
+  begin_chain(lt);
+  int rc = solve_step(0, init, lt, n_time_steps);
+  if (rc) return rc;
+  for (int step = 1; step < prm.nl; step++) {
+    rc = solve_step(step, damping_step_value(step, prm.nl, load_value), lt, 1);
+    if (rc) return rc;
+  }
+  if (total_iterations) {
+    int64_t tot = 0;
+    for (int a = 0; a < prm.nl; a++)
+      for (int t = 0; t < nts[a]; t++) tot += rec[a][t].iterations;
+    *total_iterations = tot;
+  }
   return EP2D_OK;
 }
 

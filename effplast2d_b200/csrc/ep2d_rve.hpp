@@ -84,6 +84,11 @@ class Rve {
   // ComputeEffModuli without printing (EffPlast2D.cu:179-229)
   int compute_eff_moduli(double init_load_value, const double load_type[3], int n_time_steps,
                          ep2d_result* out);
+  // ComputeEffDamping without printing (EffPlast2D.cu:230-310), nl >= 4
+  int compute_eff_damping(double init_load_value, const double load_type[3], int n_time_steps, double load_value,
+                          int64_t* total_iterations);
+  // load value of increment `step` (1 .. nl-1) of the damping chain
+  static double damping_step_value(int step, int nl, double load_value);
 
   // building blocks (used by solve_step, by the batch solver and by the tests)
   void begin_chain(const double load_type[3]);  // ComputeEffModuli's prologue
@@ -120,9 +125,10 @@ class Rve {
   bool own_stream = false;
 
   // records (EffPlast2D.h:108-117)
-  int nts[EP2D_MAX_NL] = {0, 0, 0};
-  std::vector<ep2d_step_record> rec[EP2D_MAX_NL];
-  std::vector<std::vector<double>> checks[EP2D_MAX_NL];
+  // per load step (prm.nl of them): time steps, records, checkpoint errors
+  std::vector<int> nts;
+  std::vector<std::vector<ep2d_step_record>> rec;
+  std::vector<std::vector<std::vector<double>>> checks;
   double ces[3] = {0.0, 0.0, 0.0};  // curEffStrain
   double load_type_[3] = {0.0, 0.0, 0.0};
   bool have_step0 = false;

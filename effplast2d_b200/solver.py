@@ -24,6 +24,7 @@ EXPORTS = (
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
     "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc", "ep2d_get_kernel_shape",
+    "ep2d_compute_eff_damping",
 )
 
 
@@ -73,6 +74,7 @@ def lib():
         L.ep2d_server_destroy.argtypes = [vp]
         L.ep2d_average_fields_noalloc.argtypes = [i32, i32, P(d)] + [vp] * 8
         L.ep2d_get_kernel_shape.argtypes = [vp, P(i32), P(i32)]
+        L.ep2d_compute_eff_damping.argtypes = [vp, d, P(d), i32, d, P(i64)]
         _lib = L
     return _lib
 
@@ -185,6 +187,15 @@ class Solver:
         _check(lib().ep2d_compute_eff_moduli(self._h, float(init_load_value), _dptr(lt),
                                              int(n_time_steps), ctypes.byref(res)))
         return res.as_dict()
+
+    def compute_eff_damping(self, init_load_value, load_type, n_time_steps, load_value):
+        """ComputeEffDamping (nl >= 4): returns the total iteration count; the strain and
+        stress tensors are the records of (0, n_time_steps-1) and (i, 0)."""
+        lt = np.asarray(load_type, dtype=np.float64)
+        tot = ctypes.c_int64()
+        _check(lib().ep2d_compute_eff_damping(self._h, float(init_load_value), _dptr(lt), int(n_time_steps),
+                                              float(load_value), ctypes.byref(tot)))
+        return tot.value
 
     def static_fields(self):
         nx, ny = self.nx, self.ny

@@ -28,6 +28,8 @@ extern "C" {
 
 #define EP2D_NPARS 11   /* NPARS, EffPlast2D.h:21-23 */
 #define EP2D_MAX_NL 3   /* ComputeEffModuli supports NL <= 3, EffPlast2D.cu:182-184 */
+#define EP2D_MAX_STEPS 64  /* load steps a handle keeps records for: NL >= 4 is the damping
+                              mode (ComputeEffDamping, EffPlast2D.cu:230-310) */
 
 /* status codes */
 enum {
@@ -89,7 +91,8 @@ enum {
 typedef struct ep2d_params {
   int32_t nx, ny;          /* grid; the reference uses nX = nY = 32*NGRID */
   double pa[EP2D_NPARS];   /* dX,dY,dt,K0,G0,rho0,dampX,dampY,coh,rad,N */
-  int32_t nl;              /* NL: 1 elastic, 2 + bulk increment, 3 + shear increment */
+  int32_t nl;              /* NL: 1 elastic, 2 + bulk increment, 3 + shear increment;
+                              4..EP2D_MAX_STEPS: damping mode, NL-1 sinusoidal increments */
   int32_t check_every;     /* output_step (10'000, EffPlast2D.cu:1608) */
   int64_t niter;           /* NITER */
   double eiter;            /* EITER */
@@ -242,6 +245,17 @@ int ep2d_get_check_errors(ep2d_handle* h, int32_t step, int32_t time_step,
  * of incPercent = 0.005 (EffPlast2D.h:105), then calc* (EffPlast2D.cu:1412-1539). */
 int ep2d_compute_eff_moduli(ep2d_handle* h, double init_load_value, const double load_type[3],
                             int32_t n_time_steps, ep2d_result* out);
+
+/* ComputeEffDamping (EffPlast2D.cu:230-310) without the printing: the handle's nl must be
+ * >= 4 (EP2D_ERR_ARG otherwise, as the reference throws).  Step 0 preloads
+ * init_load_value along load_type over n_time_steps; steps i = 1 .. nl-1 apply one
+ * time step each of load_value * (sin(i 2 pi' / (nl-1)) - sin((i-1) 2 pi' / (nl-1)))
+ * along load_type, pi' = 3.1415926 as the reference writes it.  The strain and stress
+ * tensors the reference prints are the records (ep2d_get_record): epsilon, epsilonPer,
+ * sigma, sigmaPer of (0, n_time_steps-1) and of (i, 0).  *total_iterations (may be
+ * NULL): iterations over all steps. */
+int ep2d_compute_eff_damping(ep2d_handle* h, double init_load_value, const double load_type[3],
+                             int32_t n_time_steps, double load_value, int64_t* total_iterations);
 
 /* SaveAnStatic2D's numerical fields (EffPlast2D.cu:1098-1134): |u| at nodes (nx*ny),
  * J1 and J2 at corners ((nx-1)*(ny-1)), from the state after the last load step with

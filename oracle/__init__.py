@@ -46,6 +46,7 @@ def lib():
         L.orc_get_record.argtypes = [vp, i32, i32, P(_abi.StepRecord)]
         L.orc_get_check_errors.argtypes = [vp, i32, i32, P(d), i32, P(i32)]
         L.orc_compute_eff_moduli.argtypes = [vp, d, P(d), i32, P(_abi.Result)]
+        L.orc_compute_eff_damping.argtypes = [vp, d, P(d), i32, d, P(ctypes.c_int64)]
         L.orc_static_fields.argtypes = [vp, d, d] + [P(d)] * 9 + [P(d)]
         L.orc_get_masks.argtypes = [vp, P(ctypes.c_uint8), P(ctypes.c_uint8)]
         _lib = L
@@ -157,6 +158,15 @@ class Oracle:
         if rc != 0:
             raise ValueError("orc_compute_eff_moduli failed with status %d" % rc)
         return res.as_dict()
+
+    def compute_eff_damping(self, init_load_value, load_type, n_time_steps, load_value):
+        lt = np.asarray(load_type, dtype=np.float64)
+        tot = ctypes.c_int64()
+        rc = lib().orc_compute_eff_damping(self._h, float(init_load_value), _dptr(lt), int(n_time_steps),
+                                           float(load_value), ctypes.byref(tot))
+        if rc != 0:
+            raise ValueError("orc_compute_eff_damping failed with status %d" % rc)
+        return tot.value
 
     def masks(self):
         node = np.zeros((self.ny, self.nx), dtype=np.uint8)

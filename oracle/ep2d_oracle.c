@@ -37,7 +37,7 @@
 #include <omp.h>
 #endif
 
-#define NSTEP_MAX EP2D_MAX_NL
+#define NSTEP_MAX EP2D_MAX_STEPS
 #define NT_MAX 64
 
 struct orc_state {
@@ -172,7 +172,7 @@ static void set_materials(orc_state* s) {
 
 int orc_create(const ep2d_params* p, orc_state** out) {
   if (!p || !out) return EP2D_ERR_ARG;
-  if (p->nx < 4 || p->ny < 4 || p->nl < 1 || p->nl > EP2D_MAX_NL || p->check_every < 1) return EP2D_ERR_ARG;
+  if (p->nx < 4 || p->ny < 4 || p->nl < 1 || p->nl > EP2D_MAX_STEPS || p->check_every < 1) return EP2D_ERR_ARG;
   orc_state* s = (orc_state*)calloc(1, sizeof(orc_state));
   if (!s) return EP2D_ERR_NOMEM;
   s->nX = p->nx;
@@ -675,10 +675,38 @@ int orc_get_check_errors(orc_state* s, int32_t step, int32_t t, double* errors, 
   return EP2D_OK;
 }
 
+/* ComputeEffDamping, EffPlast2D.cu:230-243: the preload over nTimeSteps, then NL-1
+   increments of one time step each along the same load type, of loadValue times the
+   difference of sin(i 2 pi' / (NL-1)) between consecutive steps (pi' = 3.1415926 as
+   written there).  The printed tensors (:245-297) are the records. */
+int orc_compute_eff_damping(orc_state* s, double initLoadValue, const double loadType[3], int32_t nTimeSteps,
+                            double loadValue, int64_t* total_iterations) {
+  if (!s || !loadType || nTimeSteps < 1) return EP2D_ERR_ARG;
+  if (s->nl < 4) return EP2D_ERR_ARG; /* :233-235 */
+  memcpy(s->loadType_, loadType, sizeof(s->loadType_));
+  s->an.kphi = s->an.kd = s->an.g = 0.0;
+  s->an_per = s->num = s->num_per = s->an;
+  int rc = orc_solve_step(s, 0, initLoadValue, loadType, nTimeSteps, NULL);
+  if (rc) return rc;
+  for (int i = 1; i < s->nl; i++) {
+    const double v = loadValue * (sin(i * 2.0 * 3.1415926 / (s->nl - 1)) - sin((i - 1) * 2.0 * 3.1415926 / (s->nl - 1)));
+    rc = orc_solve_step(s, i, v, loadType, 1, NULL);
+    if (rc) return rc;
+  }
+  if (total_iterations) {
+    int64_t tot = 0;
+    for (int a = 0; a < s->nl; a++)
+      for (int t = 0; t < s->nts[a]; t++) tot += s->rec[a][t].iterations;
+    *total_iterations = tot;
+  }
+  return EP2D_OK;
+}
+
 /* ComputeEffModuli, EffPlast2D.cu:179-229, and the calc and get functions, :1412-1539 */
 int orc_compute_eff_moduli(orc_state* s, double initLoadValue, const double loadType[3], int32_t nTimeSteps,
                            ep2d_result* out) {
   if (!s || !loadType || nTimeSteps < 1) return EP2D_ERR_ARG;
+  if (s->nl > EP2D_MAX_NL) return EP2D_ERR_ARG; /* EffPlast2D.cu:182-184 */
   const double incPercent = 0.005;
   memcpy(s->loadType_, loadType, sizeof(s->loadType_));
   const double sph[3] = {0.5 * (loadType[0] + loadType[1]), 0.5 * (loadType[0] + loadType[1]), 0.0};

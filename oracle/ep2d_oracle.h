@@ -31,6 +31,8 @@ int orc_solve_step(orc_state* s, int32_t step, double load_step_value, const dou
 int orc_get_record(orc_state* s, int32_t step, int32_t time_step, ep2d_step_record* out);
 int orc_get_check_errors(orc_state* s, int32_t step, int32_t time_step, double* errors_out,
                          int32_t max_n, int32_t* n_out);
+int orc_compute_eff_damping(orc_state* s, double init_load_value, const double load_type[3],
+                            int32_t n_time_steps, double load_value, int64_t* total_iterations);
 int orc_compute_eff_moduli(orc_state* s, double init_load_value, const double load_type[3],
                            int32_t n_time_steps, ep2d_result* out);
 /* SaveAnStatic2D (EffPlast2D.cu:1060-1292).  Numerical fields always; the analytic

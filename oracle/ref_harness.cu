@@ -12,7 +12,8 @@
 //       EffPlast2D.cu:389-399 launches it (grid nx/32 x ny/32, block 32x32, a device
 //       synchronisation after each launch) and writes every field to out_dir.
 //   moduli <out_dir> <initLoad> <lt.x> <lt.y> <lt.xy> <nTimeSteps> <loadValue>
-//       Runs EffPlast2D(nTimeSteps).ComputeEffModuli(...) in the current directory
+//       Runs EffPlast2D(nTimeSteps).ComputeEffModuli(...) (ComputeEffDamping(...) when the
+//       build's NL > 3, as the reference's main.cu:32-37 chooses) in the current directory
 //       (which must hold data/pa.dat), then writes the per-step records and the
 //       effective moduli at 17 significant digits (records.txt) and every device
 //       field (*.bin) to out_dir.
@@ -151,7 +152,8 @@ static int run_moduli(int argc, char** argv) {
   const unsigned nts = static_cast<unsigned>(std::stod(argv[7]));
   const double lv = std::stod(argv[8]);
   EffPlast2D e(nts);
-  e.ComputeEffModuli(init, lt, lv);
+  if (NL > 3) e.ComputeEffDamping(init, lt, lv);
+  else e.ComputeEffModuli(init, lt, lv);
   std::FILE* fp = std::fopen((out + "/records.txt").c_str(), "w");
   if (!fp) return 3;
   std::fprintf(fp, "nX %ld\nnY %ld\nNL %d\nNITER %ld\nnTimeSteps %u\n", e.nX, e.nY, (int)NL, (long)NITER, nts);

@@ -50,6 +50,8 @@ CHAIN_CASES = [
     ("c64_nl3", "g64_nl3", 64, 1, 0.01, 0.5, 1e-5, -5e-5, (1.0, 1.0, 0.5), 1),
     ("c96_nl3", "g96_nl3", 96, 3, 0.02, 0.5, 1e-5, -6e-5, (1.0, 0.8, 0.3), 2),
     ("cfg1", "cfg1", 128, 1, 0.005, 0.5, 1.0, -4e-5, (1.0, 1.0, 0.0), 1),
+    # damping mode (ComputeEffDamping, NL >= 4): preload, then 4 sinusoidal increments
+    ("c64_nl5", "g64_nl5", 64, 2, 0.02, 0.5, 1e-5, -6e-5, (1.0, 1.0, 0.2), 1),
 ]
 CFG2 = ("cfg2", "cfg2", 1024, 3, 0.01, 0.5, 1e-5, -6e-5, (1.0, 1.0, 0.0), 2)
 
@@ -61,6 +63,7 @@ MACROS = {
     "g96_nl3": dict(NGRID=3, NL=3, NITER=30000, EITER=1e-9),
     "cfg1": dict(NGRID=4, NL=1, NITER=100000, EITER=1e-9),
     "cfg2": dict(NGRID=32, NL=2, NITER=5000000, EITER=1e-9),
+    "g64_nl5": dict(NGRID=2, NL=5, NITER=20000, EITER=1e-9),
 }
 
 

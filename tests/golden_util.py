@@ -10,7 +10,7 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 KERNEL_CASES = ["k32_nl1_it1", "k32_nl3_it1", "k64x32_nl2_it1", "k64_nl3_it100", "k32x64_nl1_it100"]
-CHAIN_CASES = ["c32_nl1", "c64_nl2", "c64_nl3", "c96_nl3", "cfg1"]
+CHAIN_CASES = ["c32_nl1", "c64_nl2", "c64_nl3", "c96_nl3", "cfg1", "c64_nl5"]  # c64_nl5: damping mode (NL=5)
 
 FIELDS = ["P", "tauXX", "tauYY", "tauXY", "tauXYav", "J2", "J2XY", "Ux", "Uy", "Vx", "Vy"]
 
@@ -96,6 +96,20 @@ def same_printed(x, y, rtol, noise=1e-12):
     if abs(x) < noise and abs(y) < noise:
         return True
     return close(x, y, rtol, 1e-300)
+
+
+def tensor_tables(text):
+    """The strain / stress tensor tables ComputeEffDamping prints (EffPlast2D.cu:245-297):
+    {title: [[values of step 0], [step 1], ...]}"""
+    out, cur = {}, None
+    for line in text.splitlines():
+        if line.endswith("tensors:") or line.endswith("tensors periodic:"):
+            cur = out.setdefault(line, [])
+        elif cur is not None and re.match(r"\d+\) ", line):
+            cur.append([float(v) for v in line.split()[1:]])
+        elif cur is not None and not line.strip():
+            cur = None
+    return out
 
 
 def compare_text(mine, ref, rtol=2e-6, skip=("Calculation time",)):

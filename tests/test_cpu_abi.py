@@ -91,7 +91,7 @@ def test_solver_without_device_fails_loudly():
     assert e.value.status == _abi.ERR_NODEV
 
 
-@pytest.mark.parametrize("bad", ["nan_dx", "nl4", "tiny", "zero_pores", "kernel3", "tile_rows12", "stream_rows8",
+@pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "zero_pores", "kernel3", "tile_rows12", "stream_rows8",
                                  "stream_rows2048"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
@@ -102,8 +102,10 @@ def test_invalid_params_rejected_before_device(bad):
           "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048)}.get(bad, {})
     if bad == "nan_dx":
         pa[0] = float("nan")
-    elif bad == "nl4":
-        nl = 4
+    elif bad == "nl65":  # beyond EP2D_MAX_STEPS (nl 4..64 is the damping mode)
+        nl = 65
+    elif bad == "nl0":
+        nl = 0
     elif bad == "tiny":
         nx = 4
     elif bad == "zero_pores":

@@ -16,7 +16,8 @@ import pytest
 
 import effplast2d_b200 as ep
 from effplast2d_b200 import build as epbuild
-from golden_util import CHAIN_CASES, FIELDS, KERNEL_CASES, compare_text, field_rel_err, load
+from golden_util import (CHAIN_CASES, FIELDS, KERNEL_CASES, compare_text, field_rel_err, load, same_printed,
+                         tensor_tables)
 from test_golden_oracle import check_chain
 
 pytestmark = pytest.mark.gpu
@@ -46,7 +47,12 @@ def test_chain_vs_reference(name):
     meta, z = load(name)
     n, mac = meta["n"], meta["macros"]
     s = ep.Solver(n, n, list(z["pa"]), nl=mac["NL"], niter=mac["NITER"], eiter=mac["EITER"], check_every=10000)
-    res = s.compute_eff_moduli(meta["load"], meta["load_type"], meta["n_time_steps"])
+    if mac["NL"] >= 4:  # ComputeEffDamping; the load value is the CLI's sixth argument
+        res = {"total_iterations": s.compute_eff_damping(meta["load"], meta["load_type"], meta["n_time_steps"],
+                                                         float(meta["argv"][5]))}
+        assert res["total_iterations"] == meta["total_iterations"]
+    else:
+        res = s.compute_eff_moduli(meta["load"], meta["load_type"], meta["n_time_steps"])
     check_chain(meta, z, s, res)
     if mac["NL"] > 1:
         sf = s.static_fields()
@@ -76,6 +82,17 @@ def test_dropin_cli_vs_reference(name):
     log = open(os.path.join(work, "EffPlast2D.log")).read()
     diffs = compare_text(log, meta["cli_log"])
     assert not diffs, diffs[:5]
+    if meta["macros"]["NL"] >= 4:
+        # the damping tables go to stdout only: ours at the default 6 digits, the
+        # reference's captured at 17
+        mine_t, ref_t = tensor_tables(r.stdout), tensor_tables(meta["cli_stdout"])
+        assert sorted(mine_t) == sorted(ref_t) and len(ref_t) == 4
+        for title, rows in ref_t.items():
+            assert len(mine_t[title]) == len(rows) == meta["macros"]["NL"], title
+            for a_row, b_row in zip(mine_t[title], rows):
+                assert len(a_row) == len(b_row)
+                for a, b in zip(a_row, b_row):
+                    assert same_printed(a, b, 1e-5, noise=1e-15), (title, a_row, b_row)
     assert sorted(os.listdir(os.path.join(work, "data"))) == meta["cli_dat_files"]
     n = meta["n"]
     for f in meta["cli_dat_files"]:

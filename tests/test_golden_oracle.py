@@ -41,7 +41,11 @@ def run_chain(name):
     meta, z = load(name)
     n, mac = meta["n"], meta["macros"]
     o = oracle.Oracle(n, n, list(z["pa"]), nl=mac["NL"], niter=mac["NITER"], eiter=mac["EITER"], check_every=10000)
-    res = o.compute_eff_moduli(meta["load"], meta["load_type"], meta["n_time_steps"])
+    if mac["NL"] >= 4:  # ComputeEffDamping; the load value is the CLI's sixth argument
+        res = {"total_iterations": o.compute_eff_damping(meta["load"], meta["load_type"], meta["n_time_steps"],
+                                                         float(meta["argv"][5]))}
+    else:
+        res = o.compute_eff_moduli(meta["load"], meta["load_type"], meta["n_time_steps"])
     return meta, z, o, res
 
 
@@ -65,6 +69,10 @@ def check_chain(meta, z, solver, res, rtol_rec=1e-9, rtol_fields=1e-9):
             errs = solver.check_errors(s, t)
             for a, b in zip(errs, st["errors"]):
                 assert abs(a - b) <= 1e-5 * abs(b) + 1e-13, (s, t, a, b)
+    if nl >= 4:  # damping mode: no moduli, no Pc / tauXXc files (EffPlast2D.cu:230-310)
+        for f in ("P", "tauXX", "tauYY", "tauXY", "Ux", "Uy"):
+            assert field_rel_err(solver.get(f), z["f_" + f]) <= rtol_fields, f
+        return
     mod = meta["moduli"]
     keys = ["kphi", "kd"] + (["g"] if nl == 3 else [])
     kinds = ["num", "an"] + (["num_per", "an_per"] if (nl > 1 and meta["n_pores"] > 2) else [])
