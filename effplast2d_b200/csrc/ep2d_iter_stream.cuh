@@ -186,15 +186,25 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     take_row();
     const int r = k - 1;
 
-    // ---- trial stresses of row r
+    // ---- trial stresses of row r.  The step body is branch-free: every lane evaluates
+    // every formula (lanes a branch would mask run it in lockstep anyway) and a select
+    // keeps the value or its default, so the compiler schedules whole rows as straight
+    // code; only the stores are predicated.
     const double uyp_r = sm.ring[s_k].uy[ln1];
-    double pn = 0.0, xn = 0.0, yn = 0.0, cn = 0.0;
-    if ((INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE)) {
+    double pn, xn, yn, cn;
+    {
       const double2 kg = sm.kg[mk0 & M_MAT];
-      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), kg.x, kg.y, rdX, rdY, third, pn, xn, yn);
+      double p_, x_, y_;
+      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), kg.x, kg.y, rdX, rdY, third, p_, x_, y_);
+      const bool node_ok = (INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE);
+      pn = node_ok ? p_ : 0.0;
+      xn = node_ok ? x_ : 0.0;
+      yn = node_ok ? y_ : 0.0;
+      const double c_ =
+          corner_trial(sm.g4[g_lo | (g_hi << 2)], __dsub_rn(uxp_r, ux0_r), __dsub_rn(uyp_r, uyp), rdX, rdY);
+      const bool corner_ok = (INTERIOR || (i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1)) && !(mk0 & M_CORNER);
+      cn = corner_ok ? c_ : 0.0;
     }
-    if ((INTERIOR || (i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1)) && !(mk0 & M_CORNER))
-      cn = corner_trial(sm.g4[g_lo | (g_hi << 2)], __dsub_rn(uxp_r, ux0_r), __dsub_rn(uyp_r, uyp), rdX, rdY);
     const double xa_r = xb_r, ya_r = yb_r;
     pa_ = pb; xa = xb; ya = yb;
     pb = pn; xb = xn; yb = yn;
@@ -222,23 +232,22 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
         c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
       }
-      double fn = 1.0, fc = 1.0;
-      if (INTERIOR || (coln && j >= 0 && j < ny)) {
-        const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
-        const double J2sq = node_j2sq(xa, ya, tav);
-        fn = return_factor(J2sq, coh, coh2);
-        if (RECORD) {
-          tav_o = __dmul_rn(tav, fn);
-          j2_o = (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o)) : __dsqrt_rn(J2sq);
-        }
-      }
+      const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
+      const double nJ2sq = node_j2sq(xa, ya, tav);
+      const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
+      const double fn = node_in ? return_factor(nJ2sq, coh, coh2) : 1.0;
       // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
-      if (INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1)) {
-        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
-        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
-        const double J2sq = corner_j2sq(sx, sy, c2);
-        fc = return_factor(J2sq, coh, coh2);
-        if (RECORD) j2xy_o = __dsqrt_rn(J2sq);
+      const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
+      const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
+      const double cJ2sq = corner_j2sq(sx, sy, c2);
+      const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
+      const double fc = corner_in ? return_factor(cJ2sq, coh, coh2) : 1.0;
+      if (RECORD) {
+        tav_o = node_in ? __dmul_rn(tav, fn) : 0.0;
+        j2_o = !node_in ? 0.0
+                        : (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o))
+                                      : __dsqrt_rn(nJ2sq);
+        j2xy_o = corner_in ? __dsqrt_rn(cJ2sq) : 0.0;
       }
       xr = __dmul_rn(xa, fn);
       yr = __dmul_rn(ya, fn);
@@ -249,51 +258,48 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     pw = pa_; xw = xr; yw = yr; cw = cr;
     cw_l = shfl_up1(cw);
 
-    // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring
+    // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring.  A face
+    // the reference leaves alone gets its old velocity back, unchanged.
     const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
-    if (j >= jA && own) {
+    if (j >= jA) {
       const StreamRow<TV>& rj = sm.ring[s_k2];
       const double uxm = rj.ux[lane], uym = rj.uy[lane];
       const double vxm = (double)rj.vx[lane], vym = (double)rj.vy[lane];
-      const int q = j * pitch + i;
-      double vx = vxm;
-      if (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) {
-        vx = face_velocity(vx, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, __dsub_rn(cw_l, cq_l), rdY);
-        const TV vs = (TV)vx;
-        fvx[q] = vs;
-        vx = (double)vs;  // the displacement moves by the stored velocity
-      }
-      uxo[q] = advance(uxm, vx, dT);
-      double vy = vym;
-      if (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) {
-        vy = face_velocity(vy, cY, dtr, face_diff(pw, pq, yw, yq), rdY, __dsub_rn(cq, cq_l), rdX);
-        const TV vs = (TV)vy;
-        fvy[q] = vs;
-        vy = (double)vs;
-      }
-      uyo[q] = advance(uym, vy, dT);
-      if (!INTERIOR) {
-        if (i == nx - 1) {  // face column nx of Ux/Vx (lane + 1): never updated
-          uxo[j * pitch + nx] = rj.ux[lane + 1];
-          if (RECORD) vmx = fmax(vmx, fabs((double)rj.vx[lane + 1]));
+      const TV vxs = (TV)face_velocity(vxm, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, __dsub_rn(cw_l, cq_l), rdY);
+      const TV vys = (TV)face_velocity(vym, cY, dtr, face_diff(pw, pq, yw, yq), rdY, __dsub_rn(cq, cq_l), rdX);
+      // the displacement moves by the stored velocity
+      const double vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (double)vxs : vxm;
+      const double vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (double)vys : vym;
+      const double uxn = advance(uxm, vx, dT), uyn = advance(uym, vy, dT);
+      if (own) {
+        const int q = j * pitch + i;
+        fvx[q] = (TV)vx;
+        fvy[q] = (TV)vy;
+        uxo[q] = uxn;
+        uyo[q] = uyn;
+        if (!INTERIOR) {
+          if (i == nx - 1) {  // face column nx of Ux/Vx (lane + 1): never updated
+            uxo[j * pitch + nx] = rj.ux[lane + 1];
+            if (RECORD) vmx = fmax(vmx, fabs((double)rj.vx[lane + 1]));
+          }
+          if (j == ny - 1) {  // face row ny of Uy/Vy (row k-1 of the ring): never updated
+            const StreamRow<TV>& rj1 = sm.ring[s_k1];
+            uyo[ny * pitch + i] = rj1.uy[lane];
+            if (RECORD) vmy = fmax(vmy, fabs((double)rj1.vy[lane]));
+          }
         }
-        if (j == ny - 1) {  // face row ny of Uy/Vy (row k-1 of the ring): never updated
-          const StreamRow<TV>& rj1 = sm.ring[s_k1];
-          uyo[ny * pitch + i] = rj1.uy[lane];
-          if (RECORD) vmy = fmax(vmy, fabs((double)rj1.vy[lane]));
-        }
-      }
-      if (RECORD) {
-        vmx = fmax(vmx, fabs(vx));
-        vmy = fmax(vmy, fabs(vy));
-        f.p[q] = pw;
-        f.txx[q] = xw;
-        f.tyy[q] = yw;
-        if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.txy[q] = cw;
-        if (PLASTIC) {
-          f.txyav[q] = tav_o;
-          f.j2[q] = j2_o;
-          if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.j2xy[q] = j2xy_o;
+        if (RECORD) {
+          vmx = fmax(vmx, fabs(vx));
+          vmy = fmax(vmy, fabs(vy));
+          f.p[q] = pw;
+          f.txx[q] = xw;
+          f.tyy[q] = yw;
+          if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.txy[q] = cw;
+          if (PLASTIC) {
+            f.txyav[q] = tav_o;
+            f.j2[q] = j2_o;
+            if (INTERIOR || (i < nx - 1 && j < ny - 1)) f.j2xy[q] = j2xy_o;
+          }
         }
       }
     }
