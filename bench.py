@@ -493,6 +493,40 @@ def run_batch(args):
     return 0
 
 
+def run_precision(args):
+    """The mixed-precision path (FP32 velocity storage) against the plain FP64 path on one
+    workload, both solved to convergence through the whole ComputeEffModuli chain: the
+    relative error of every modulus, iteration counts and solve times."""
+    import math
+
+    import effplast2d_b200 as ep
+
+    w = WORKLOADS[args.precision_workload]
+    n = w["n"]
+    pa = make_pa(w)
+    out = {}
+    for name, prec in (("fp64", ep.FP64), ("mixed", ep.MIXED)):
+        s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
+                      precision=prec)
+        t = time.perf_counter()
+        res = s.compute_eff_moduli(w["load"], list(w["load_type"]), w["n_time_steps"])
+        out[name] = {"seconds": time.perf_counter() - t, "total_iterations": res["total_iterations"],
+                     "all_converged": bool(res["all_converged"]), "num": res["num"], "num_per": res["num_per"],
+                     "kernel_us": 1000 * s.stats()["kernel_ms"] / max(s.stats()["launches"], 1)}
+        s.close()
+    err = {}
+    for kind in ("num", "num_per"):
+        for k in ("kphi", "kd", "g"):
+            a, b = out["mixed"][kind][k], out["fp64"][kind][k]
+            if math.isfinite(a) and math.isfinite(b) and b != 0.0:
+                err["%s_%s" % (kind, k)] = abs(a - b) / abs(b)
+            else:
+                err["%s_%s" % (kind, k)] = None  # undefined in both (e.g. G without shear)
+    print(json.dumps({"workload": "precision", "config": args.precision_workload, "description": w["label"],
+                      "relative_error_mixed_vs_fp64": err, "runs": out}))
+    return 0
+
+
 def run_serve(args):
     """Poisson stream of requests into the continuous-batching server: p50/p99 latency
     and solves/s, with the plain FP64 one-at-a-time path's solves/s beside them."""
@@ -539,7 +573,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve", "precision"])
+    ap.add_argument("--precision-workload", default="cfg3", choices=sorted(WORKLOADS),
+                    help="workload of --workload precision (mixed vs FP64 moduli)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-solves", type=int, default=1,
@@ -547,6 +583,8 @@ def main():
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "precision":
+        return run_precision(args)
     if args.workload == "serve":
         return run_serve(args)
     w = WORKLOADS[args.workload]
