@@ -199,6 +199,12 @@ int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t
   return EP2D_OK;
 }
 
+int ep2d_polar_fields(ep2d_handle* h, double load_value, double* snu_rr, double* snu_ff, double* san_rr,
+                      double* san_ff, uint8_t* plastic) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  EP2D_GUARD({ return h->rve.polar_fields(load_value, snu_rr, snu_ff, san_rr, san_ff, plastic); })
+}
+
 int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
   if (kernel) *kernel = h->rve.shape.form == ep2d::FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;

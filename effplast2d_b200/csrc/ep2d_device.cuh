@@ -307,6 +307,54 @@ __global__ void k_static_fields(Geo g, const double* __restrict__ Ux, const doub
 }
 
 
+// The plastic-zone map and the stresses in polar coordinates around the centre that
+// get_sigma_2D.m:170-194 computes after its solve, here from the recorded final state.
+// plastic = (node yields) + (yielding corners among the four around the node), as
+// Plast + PlastXY there; a node yields if its recorded (returned) J2 reached coh (to
+// 1e-12 relative), a corner if its recorded trial J2XY exceeds coh.  In the plastic zone
+// (plastic > 0): the numerical sigma_rr, sigma_phiphi from tauXX - P, tauYY - P and
+// tauXYav rotated to polar axes, and the analytic ones
+// -P0 + sign(load) 2 coh (log(sqrt(r)) [+ 1]) / sqrt(2), P0 = 0; zero elsewhere and
+// inside the pore (r < rad).  Output unpadded, node (i, j) at j*nx + i.
+__global__ void k_polar_fields(Geo g, const double* __restrict__ P, const double* __restrict__ txx,
+                               const double* __restrict__ tyy, const double* __restrict__ txyav,
+                               const double* __restrict__ j2, const double* __restrict__ j2xy, double sgn,
+                               double* __restrict__ snrr, double* __restrict__ snff, double* __restrict__ sarr,
+                               double* __restrict__ saff, uint8_t* __restrict__ plast) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny;
+  if (i >= nx || j >= ny) return;
+  const size_t pitch = (size_t)g.pitch, q = j * pitch + i;
+  const double coh = g.coh;
+  int count = (j2[q] >= coh * (1.0 - 1e-12)) ? 1 : 0;
+  for (int dj = -1; dj <= 0; dj++)
+    for (int di = -1; di <= 0; di++) {
+      const int ci = i + di, cj = j + dj;
+      if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1 && j2xy[cj * pitch + ci] > coh) count++;
+    }
+  const double x = -0.5 * g.dX * (nx - 1) + g.dX * i;
+  const double y = -0.5 * g.dY * (ny - 1) + g.dY * j;
+  const double r = sqrt(x * x + y * y);
+  const double s = y / r, c = x / r;
+  const double sxx = txx[q] - P[q], syy = tyy[q] - P[q], sxy = txyav[q];
+  double a = 0.0, b = 0.0, ar = 0.0, af = 0.0;
+  if (count > 0) {
+    a = sxx * c * c + 2.0 * sxy * s * c + syy * s * s;
+    b = sxx * s * s - 2.0 * sxy * s * c + syy * c * c;
+    const double lg = log(sqrt(r));
+    ar = sgn * 2.0 * coh * lg / sqrt(2.0);
+    af = sgn * 2.0 * coh * (lg + 1.0) / sqrt(2.0);
+  }
+  if (r < g.rad) a = b = ar = af = 0.0;
+  const size_t o = (size_t)j * nx + i;
+  snrr[o] = a;
+  snff[o] = b;
+  sarr[o] = ar;
+  saff[o] = af;
+  plast[o] = (uint8_t)count;
+}
+
 // ---------------------------------------------------------------------------------
 // Analytic static solution and error maps (SaveAnStatic2D, EffPlast2D.cu:1060-1292;
 // getAnalytic* :989-1059).  Complex FP64 on the device.  The complex helpers follow the

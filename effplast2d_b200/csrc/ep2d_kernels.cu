@@ -238,6 +238,15 @@ cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double*
   return cudaGetLastError();
 }
 
+cudaError_t launch_polar_fields(const Geo& g, const Fields& f, double sgn, double* snrr, double* snff, double* sarr,
+                                double* saff, uint8_t* plast, cudaStream_t stream) {
+  const dim3 block(32, 8);
+  const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
+  k_polar_fields<<<grid, block, 0, stream>>>(g, f.p, f.txx, f.tyy, f.txyav, f.j2, f.j2xy, sgn, snrr, snff, sarr, saff,
+                                             plast);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_analytic(const Geo& g, const AnParams& a, const double* unu, const double* j1nu, const double* j2nu,
                             double* uan, double* eu, double* j1an, double* j2an, double* ej1, double* ej2,
                             double* stats, cudaStream_t stream) {

@@ -856,6 +856,28 @@ int Rve::static_fields(double* unu, double* j1, double* j2) {
   return EP2D_OK;
 }
 
+int Rve::polar_fields(double load_value, double* snrr, double* snff, double* sarr, double* saff, uint8_t* plast) {
+  if (!snrr || !snff || !sarr || !saff || !plast) return fail(EP2D_ERR_ARG, "null output buffer");
+  DeviceScope ds(device);
+  const size_t nn = (size_t)prm.nx * prm.ny;
+  // sign(loadValue), get_sigma_2D.m:175 (MATLAB sign: 0 for 0)
+  const double sgn = load_value > 0.0 ? 1.0 : (load_value < 0.0 ? -1.0 : 0.0);
+  double* tmp = nullptr;
+  EP2D_CK(cudaMallocAsync(&tmp, 4 * nn * sizeof(double) + nn, stream));
+  uint8_t* pl = reinterpret_cast<uint8_t*>(tmp + 4 * nn);
+  cudaError_t e = launch_polar_fields(g, f, sgn, tmp, tmp + nn, tmp + 2 * nn, tmp + 3 * nn, pl, stream);
+  double* outs[4] = {snrr, snff, sarr, saff};
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaMemcpyAsync(outs[k], tmp + k * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(plast, pl, nn, cudaMemcpyDeviceToHost, stream);
+  cudaFreeAsync(tmp, stream);
+  cudaError_t se = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess || se != cudaSuccess)
+    return fail(EP2D_ERR_CUDA, std::string("polar fields: ") + cudaGetErrorString(e != cudaSuccess ? e : se));
+  aux_launches += 1;
+  return EP2D_OK;
+}
+
 int Rve::analytic_fields(double deltaP, double tauInfty, double* uan, double* eu, double* j1an, double* j2an,
                          double* ej1, double* ej2, double stats[6]) {
   if (!uan || !eu || !j1an || !j2an || !ej1 || !ej2 || !stats) return fail(EP2D_ERR_ARG, "null output buffer");

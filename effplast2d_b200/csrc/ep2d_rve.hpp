@@ -108,6 +108,8 @@ class Rve {
   int get_field(int field, double* host) const;
   int set_field(int field, const double* host);
   int static_fields(double* unu, double* j1, double* j2);
+  // get_sigma_2D.m:170-194's plastic zone and polar stresses from the recorded state
+  int polar_fields(double load_value, double* snrr, double* snff, double* sarr, double* saff, uint8_t* plast);
   // SaveAnStatic2D's analytic fields and error statistics (EffPlast2D.cu:1060-1292)
   int analytic_fields(double delta_p, double tau_infty, double* uan, double* eu, double* j1an, double* j2an,
                       double* ej1, double* ej2, double stats[6]);

@@ -93,6 +93,8 @@ cudaError_t launch_gather(const Geo& g, const Fields& f, int src, const unsigned
                           double* out, cudaStream_t stream);
 cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double* unu, double* j1, double* j2,
                                  cudaStream_t stream);
+cudaError_t launch_polar_fields(const Geo& g, const Fields& f, double sgn, double* snrr, double* snff, double* sarr,
+                                double* saff, uint8_t* plast, cudaStream_t stream);
 
 // Scalars of the analytic static solution (SaveAnStatic2D, EffPlast2D.cu:1062-1078).
 struct AnParams {

@@ -24,7 +24,7 @@ EXPORTS = (
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
     "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc", "ep2d_get_kernel_shape",
-    "ep2d_compute_eff_damping",
+    "ep2d_compute_eff_damping", "ep2d_polar_fields",
 )
 
 
@@ -75,6 +75,7 @@ def lib():
         L.ep2d_average_fields_noalloc.argtypes = [i32, i32, P(d)] + [vp] * 8
         L.ep2d_get_kernel_shape.argtypes = [vp, P(i32), P(i32)]
         L.ep2d_compute_eff_damping.argtypes = [vp, d, P(d), i32, d, P(i64)]
+        L.ep2d_polar_fields.argtypes = [vp, d] + [P(d)] * 4 + [P(ctypes.c_uint8)]
         _lib = L
     return _lib
 
@@ -204,6 +205,18 @@ class Solver:
         j2 = np.zeros((ny - 1, nx - 1))
         _check(lib().ep2d_static_fields(self._h, _dptr(unu), _dptr(j1), _dptr(j2)))
         return {"UnuAbs": unu, "J1nu": j1, "J2nu": j2}
+
+    def polar_fields(self, load_value):
+        """get_sigma_2D.m:170-194 on the recorded state: dict of Snurr, Snuff, Sanrr, Sanff
+        ((ny, nx) doubles) and Plast ((ny, nx) uint8 counts)."""
+        nx, ny = self.nx, self.ny
+        out = {k: np.zeros((ny, nx)) for k in ("Snurr", "Snuff", "Sanrr", "Sanff")}
+        pl = np.zeros((ny, nx), dtype=np.uint8)
+        _check(lib().ep2d_polar_fields(self._h, float(load_value), *[_dptr(out[k]) for k in
+                                                                     ("Snurr", "Snuff", "Sanrr", "Sanff")],
+                                       pl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        out["Plast"] = pl
+        return out
 
     def analytic_fields(self, delta_p, tau_infty):
         nx, ny = self.nx, self.ny

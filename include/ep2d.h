@@ -273,6 +273,22 @@ int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, doubl
                          double* error_uabs, double* j1an, double* j2an, double* error_j1,
                          double* error_j2, double stats[6]);
 
+/* The plastic zone and the stresses in polar coordinates about the grid centre (the pore
+ * of a single-pore RVE) that the reference's CPU solver computes after its solve
+ * (get_sigma_2D.m:170-194), here from the state the last iteration recorded.  Every
+ * output is nx*ny, node (i, j) at j*nx + i:
+ *   plastic: 1 if the node yields (recorded J2 reached coh) plus the number of yielding
+ *            corners (recorded trial J2XY > coh) among the four around it, as
+ *            Plast + PlastXY there; the reference's CPU solver counts a node or corner
+ *            that yielded at any iteration, this the final state's;
+ *   snu_rr, snu_ff: tauXX - P, tauYY - P, tauXYav rotated to the polar axes, where
+ *            plastic > 0;
+ *   san_rr, san_ff: -P0 + sign(load_value) 2 coh (log(sqrt(r)) [+ 1]) / sqrt(2), P0 = 0,
+ *            where plastic > 0;
+ * all zero elsewhere and inside the pore (r < rad). */
+int ep2d_polar_fields(ep2d_handle* h, double load_value, double* snu_rr, double* snu_ff, double* san_rr,
+                      double* san_ff, uint8_t* plastic);
+
 /* ---- batch ---------------------------------------------------------------------- */
 /* Solve n RVEs together: every RVE runs ComputeEffModuli's chain (EffPlast2D.cu:179-229)
  * with the reference's convergence test and checkpoint cadence; all active RVEs advance

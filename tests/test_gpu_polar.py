@@ -1,0 +1,57 @@
+"""The plastic zone and polar stresses of get_sigma_2D.m:170-194 (ep2d_polar_fields)
+against a numpy restatement of those lines applied to the solver's own recorded fields.
+The reference's CPU solver cannot run here (no MATLAB or Octave), so this pins the
+arithmetic, not the CPU solver's trajectory."""
+import numpy as np
+import pytest
+
+import effplast2d_b200 as ep
+
+pytestmark = pytest.mark.gpu
+
+
+def polar_numpy(s, pa, load_value):
+    nx, ny = s.nx, s.ny
+    dX, dY, coh, rad = pa[0], pa[1], pa[8], pa[9]
+    P, txx, tyy, tav = s.get("P"), s.get("tauXX"), s.get("tauYY"), s.get("tauXYav")
+    j2, j2xy = s.get("J2"), s.get("J2XY")
+    plast = (j2 >= coh * (1.0 - 1e-12)).astype(np.int64)
+    pxy = (j2xy > coh).astype(np.int64)
+    # Plast(1:end-1,1:end-1) += PlastXY, etc. (get_sigma_2D.m:170-173)
+    plast[:-1, :-1] += pxy
+    plast[1:, :-1] += pxy
+    plast[:-1, 1:] += pxy
+    plast[1:, 1:] += pxy
+    x = (-0.5 * dX * (nx - 1) + dX * np.arange(nx))[None, :]
+    y = (-0.5 * dY * (ny - 1) + dY * np.arange(ny))[:, None]
+    r = np.sqrt(x * x + y * y)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        sn, cs = y / r, x / r
+        pz = plast > 0
+        snrr = np.where(pz, (txx - P) * cs * cs + 2.0 * tav * sn * cs + (tyy - P) * sn * sn, 0.0)
+        snff = np.where(pz, (txx - P) * sn * sn - 2.0 * tav * sn * cs + (tyy - P) * cs * cs, 0.0)
+        lg = np.log(np.sqrt(r))
+        sarr = np.where(pz, np.sign(load_value) * 2.0 * coh * lg / np.sqrt(2.0), 0.0)
+        saff = np.where(pz, np.sign(load_value) * 2.0 * coh * (lg + 1.0) / np.sqrt(2.0), 0.0)
+    inside = r < rad
+    for a in (snrr, snff, sarr, saff):
+        a[inside] = 0.0
+    return {"Plast": plast, "Snurr": snrr, "Snuff": snff, "Sanrr": sarr, "Sanff": saff}
+
+
+@pytest.mark.parametrize("n,nl,lt", [(96, 3, (1.0, 1.0, 0.0)), (128, 2, (1.0, 0.8, 0.2)), (64, 1, (1.0, 1.0, 0.0))])
+def test_polar_fields_match_restatement(n, nl, lt):
+    load = -6e-5
+    pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=1e-5 if nl > 1 else 1.0, porosity=0.02, n_pores=1)
+    s = ep.Solver(n, n, pa, nl=nl, niter=20000, eiter=1e-9, check_every=10000)
+    s.compute_eff_moduli(load, list(lt), 1)
+    got = s.polar_fields(load)
+    ref = polar_numpy(s, pa, load)
+    assert np.array_equal(got["Plast"].astype(np.int64), ref["Plast"])
+    if nl > 1:
+        assert (got["Plast"] > 0).mean() > 0.01  # a plastic zone around the pore
+    else:
+        assert not got["Plast"].any()
+    for k in ("Snurr", "Snuff", "Sanrr", "Sanff"):
+        scale = max(np.max(np.abs(ref[k])), 1e-300)
+        assert np.max(np.abs(got[k] - ref[k])) <= 1e-12 * scale, k
