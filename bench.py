@@ -102,6 +102,11 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's start-up (NVML initialisation) must not fall inside the timed
+        # region: wait for its first sample
+        t = time.time()
+        while not self.rows and time.time() - t < 5.0 and self.proc.poll() is None:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
