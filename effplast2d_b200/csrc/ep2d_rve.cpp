@@ -90,6 +90,13 @@ IterShape shape_of(const ep2d_params& p, int sm_count) {
     const int64_t strips = (p.nx + STREAM_COLS - 1) / STREAM_COLS;
     s.rows = 64;
     while (s.rows > SEG_MIN && strips * ((p.ny + s.rows - 1) / s.rows) < 16 * (int64_t)sm_count) s.rows /= 2;
+    // too few segments to keep 6 warps on every SM (grids up to ~600^2): a warp's march
+    // latency then sets the iteration time, and the tile form, one thread per cell, is
+    // faster (256^2: 7 vs 14 us; 512^2: 10 vs 15 us).  Both forms round alike.
+    if (p.kernel == EP2D_KERNEL_AUTO && strips * ((p.ny + SEG_MIN - 1) / SEG_MIN) < 6 * (int64_t)sm_count) {
+      s.form = FORM_TILE;
+      s.rows = TILE_Y;
+    }
   }
   return s;
 }

@@ -54,8 +54,9 @@ void final_moduli(int nl, const ep2d_step_record& r0, const ep2d_step_record* r1
 int validate_params(const ep2d_params& p);
 // The iteration kernel a handle uses: the form and rows the parameters name, or the
 // library's choice where they are 0: the stream form, with the tallest segments (64,
-// 32 or 16 rows) that still give every SM of the device 16 warps' worth of segments
-// (sm_count <= 0: SEG_DEFAULT rows).
+// 32 or 16 rows) that still give every SM of the device 16 warps' worth of segments, or
+// the tile form (16 rows) when 16-row segments would leave fewer than 6 warps per SM
+// (sm_count <= 0: stream form, SEG_DEFAULT rows).
 IterShape shape_of(const ep2d_params& p, int sm_count = 0);
 
 // Device row pitch (elements) for an nx-wide grid.
