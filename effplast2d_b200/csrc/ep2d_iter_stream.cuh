@@ -10,8 +10,9 @@
 //   returns row r-1 (node: tauXY averaged onto the node from the clamped 2x2 corner
 //           block; corner: tauXX, tauYY averaged onto the corner),
 //   updates the faces of row r-1 (damped momentum, U += V dt).
-// Rows reach the ring by cp.async, STREAM_DEPTH rows ahead of use, so each warp keeps
-// that many rows of loads in flight without holding them in registers: the march is a
+// Rows reach the ring by cp.async (U and V as 16-byte column pairs), STREAM_DEPTH rows
+// ahead of use, so each warp keeps that many rows of loads in flight without holding
+// them in registers: the march is a
 // chain of dependent steps, and without the ring a warp would wait one memory latency
 // per row.  Neighbouring columns come from warp shuffles; a value a step needs from a
 // neighbour that the previous step already fetched (the same quantity one row lower)
@@ -65,13 +66,20 @@ __device__ __forceinline__ double shfl_dn(double v) { return __shfl_down_sync(0x
 __device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ int shfl_dn_i(int v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-// cp.async of 4 or 8 bytes; with ok == false nothing is read and the destination is
+// cp.async of 4, 8 or 16 bytes; with ok == false nothing is read and the destination is
 // zero-filled (src-size 0), `src` then only has to be a valid address.
 template <int BYTES>
 __device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, bool ok) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES), "r"(ok ? BYTES : 0)
                : "memory");
+}
+// two consecutive elements of a field: 16 bytes (double) or 8 (float).  Through L1
+// (.ca): neighbouring strips share their halo columns there; the L2-only form (.cg) ran
+// 4 % slower at 2048^2.
+template <typename T>
+__device__ __forceinline__ void cp_async_pair_zfill(T* dst, const T* src, bool ok) {
+  cp_async_zfill<(int)(2 * sizeof(T))>(dst, src, ok);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -103,26 +111,33 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   TV* __restrict__ fvy = static_cast<TV*>(f.vy);
   const uint8_t* __restrict__ mask = f.mask;
 
-  const bool colx = INTERIOR || (i >= 0 && i <= nx);  // column of Ux / Vx
   const bool coln = INTERIOR || (i >= 0 && i < nx);   // column of nodes, Uy, Vy
   const int mshift = 8 * (i & 3);                     // pitch % 32 == 0: byte i & 3 of the word
   const int ln1 = min(lane + 1, 31);                  // the lane of column i + 1 (lane 31: unused)
   const int mshift1 = 8 * ((i + 1) & 3);
 
   // rows k_first .. k_last pass through the ring: U and the mask are needed up to row
-  // r + 1 and V up to row r for steps r = jA - 2 .. jB
+  // r + 1 and V up to row r for steps r = jA - 2 .. jB.  U and V move in column pairs:
+  // lanes 0..15 copy the 16 pairs of the warp's 32 columns of Ux (Vx), lanes 16..31
+  // those of Uy (Vy), 16 (V as float: 8) bytes each; a pair starts on an even column at
+  // a 16-byte aligned address (pitch % 32 == 0) and lies in its row as long as it starts
+  // inside the pitch.  Columns past the grid read the row padding, which nothing writes
+  // and which holds zeros, like the zero fill of rows and columns outside the arrays.
   const int k_first = jA - 3, k_last = jB + 1;
+  const int half = lane >> 4;                                  // 0: Ux, Vx; 1: Uy, Vy
+  const int pc = STREAM_COLS * strip - 2 + 2 * (lane & 15);    // first column of the pair
+  const bool pair_in = INTERIOR || (pc >= 0 && pc < pitch);
+  const int rows_of = half ? ny + 1 : ny;                      // Uy, Vy: rows 0 .. ny
+  const double* __restrict__ u_src = half ? uy : ux;
+  const TV* __restrict__ v_src = half ? fvy : fvx;
   auto issue = [&](int k, int slot) {
     StreamRow<TV>& row = sm.ring[slot];
-    const bool rx = INTERIOR || (colx && k >= 0 && k < ny);   // Ux, Vx: rows 0 .. ny-1
-    const bool ry = INTERIOR || (coln && k >= 0 && k <= ny);  // Uy, Vy: rows 0 .. ny
-    const bool rm = INTERIOR || (coln && k >= 0 && k < ny);   // nodes
-    const int q = (rx || ry) ? k * pitch + i : 0;
-    cp_async_zfill<8>(&row.ux[lane], ux + (rx ? q : 0), rx);
-    cp_async_zfill<8>(&row.uy[lane], uy + (ry ? q : 0), ry);
-    cp_async_zfill<(int)sizeof(TV)>(&row.vx[lane], fvx + (rx ? q : 0), rx);
-    cp_async_zfill<(int)sizeof(TV)>(&row.vy[lane], fvy + (ry ? q : 0), ry);
-    cp_async_zfill<4>(&row.m[lane], mask + (rm ? (q & ~3) : 0), rm);
+    const bool ok = pair_in && (INTERIOR || (k >= 0 && k < rows_of));
+    const int q = ok ? k * pitch + pc : 0;
+    cp_async_pair_zfill<double>((half ? row.uy : row.ux) + 2 * (lane & 15), u_src + q, ok);
+    cp_async_pair_zfill<TV>((half ? row.vy : row.vx) + 2 * (lane & 15), v_src + q, ok);
+    const bool rm = INTERIOR || (coln && k >= 0 && k < ny);  // nodes
+    cp_async_zfill<4>(&row.m[lane], mask + (rm ? ((k * pitch + i) & ~3) : 0), rm);
   };
   int slot_wr = 0;
 #pragma unroll 1
