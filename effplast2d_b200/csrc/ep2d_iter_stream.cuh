@@ -139,14 +139,6 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     const bool rm = INTERIOR || (coln && k >= 0 && k < ny);  // nodes
     cp_async_zfill<4>(&row.m[lane], mask + (rm ? ((k * pitch + i) & ~3) : 0), rm);
   };
-  int slot_wr = 0;
-#pragma unroll 1
-  for (int d = 0; d < STREAM_DEPTH; d++) {
-    if (k_first + d <= k_last) issue(k_first + d, slot_wr);
-    cp_async_commit();  // empty groups keep the count uniform
-    slot_wr++;
-  }
-
   const double rdX = g.rdX, rdY = g.rdY, third = 1.0 / 3.0;
   const double coh = g.coh, coh2 = g.coh2;
   const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
@@ -154,6 +146,19 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   if (lane < 16) sm.g4[lane] = corner_g4_of_bits(lane, g.G0, g.Gp);
   if (lane < 2) sm.kg[lane] = make_double2(lane ? g.Kp : g.K0, __dmul_rn(2.0, lane ? g.Gp : g.G0));
   __syncwarp();
+
+  // Launched as a programmatic dependent of the previous iteration (single-RVE form),
+  // this kernel may start before that one has finished; nothing above touches global
+  // memory.  Wait for the previous grid to complete (its stores visible) before the
+  // first load; without such a launch (the batched form) the wait returns at once.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  int slot_wr = 0;
+#pragma unroll 1
+  for (int d = 0; d < STREAM_DEPTH; d++) {
+    if (k_first + d <= k_last) issue(k_first + d, slot_wr);
+    cp_async_commit();  // empty groups keep the count uniform
+    slot_wr++;
+  }
 
   // registers at step r (suffix _r: column i+1, _l: column i-1): U rows r (0) and r+1
   // (p), masks rows r and r+1; U and V of row r-1 and r are read back from the ring
@@ -352,6 +357,9 @@ __global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream(Geo g, Fields
                                                                    int seg_h) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   StreamWarpSmem<TV>& sm = reinterpret_cast<StreamWarpSmem<TV>*>(smem_raw)[threadIdx.x >> 5];
+  // let the next iteration's grid be scheduled now: it waits for this grid's completion
+  // before reading anything (griddepcontrol.wait in stream_task)
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const int task = blockIdx.x * STREAM_WARPS + (threadIdx.x >> 5);
   if (task >= nstrips * nsegs) return;  // whole warp
   double vmx = 0.0, vmy = 0.0;
