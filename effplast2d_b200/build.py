@@ -72,6 +72,19 @@ DROPIN = os.path.join(CSRC, "dropin")
 CLI = os.path.join(HERE, "ep2d_cli")
 
 
+def build_cli_unity(macros, out, force=False):
+    """The self-contained drop-in CLI: the reference's nvcc line plus -DEP2D_UNITY, the
+    library sources compiled into the binary (no libep2d.so needed at run time)."""
+    srcs = [os.path.join(DROPIN, s) for s in ("EffPlast2D.cu", "main.cu")]
+    deps = srcs + [os.path.join(DROPIN, "EffPlast2D.h")] + [os.path.join(CSRC, h) for h in HEADERS] + \
+        [os.path.join(CSRC, s) for s in ("ep2d_kernels.cu", "ep2d_rve.cpp", "ep2d_api.cpp")]
+    if force or _newer(out, deps):
+        flags = ["-D%s=%s" % (k, v) for k, v in macros.items()]
+        _run([NVCC, "-O3", "-std=c++17", *ARCH, "-DEP2D_UNITY", *flags, "-I" + INCLUDE, "-I" + CSRC, "-o", out,
+              *srcs])
+    return out
+
+
 def build_cli(macros=None, out=None, force=False):
     """Build the drop-in CLI (the reference's main.cu + EffPlast2D class contract) from
     csrc/dropin with the reference's compile-time macros (NL, NGRID, NITER, EITER,

@@ -108,6 +108,27 @@ def test_dropin_cli_vs_reference(name):
             assert field_rel_err(mine, ref) <= tol, f
 
 
+def test_dropin_unity_build_vs_reference():
+    # the self-contained build INTEGRATION.md gives (library sources compiled into the
+    # binary with -DEP2D_UNITY): same log and .dat files as the reference's
+    name = "c64_nl2"
+    meta, z = load(name)
+    exe = epbuild.build_cli_unity(meta["macros"] | {"NPARS": 11, "DEVICE_IDX": 0},
+                                  os.path.join(epbuild.BUILD, "cli_unity_" + name))
+    work = tempfile.mkdtemp()
+    os.makedirs(os.path.join(work, "data"))
+    np.asarray(z["pa"], dtype="<f8").tofile(os.path.join(work, "data", "pa.dat"))
+    r = subprocess.run([exe] + meta["argv"], cwd=work, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    diffs = compare_text(open(os.path.join(work, "EffPlast2D.log")).read(), meta["cli_log"])
+    assert not diffs, diffs[:5]
+    assert sorted(os.listdir(os.path.join(work, "data"))) == meta["cli_dat_files"]
+    n = meta["n"]
+    mine = np.fromfile(os.path.join(work, "data", "Pc_%d_.dat" % n), dtype="<f8")
+    assert field_rel_err(mine, z["dat_Pc_%d_.dat" % n]) <= 1e-9
+
+
 def test_dropin_cli_error_paths():
     exe = cli_for("c32_nl1")
     work = tempfile.mkdtemp()
