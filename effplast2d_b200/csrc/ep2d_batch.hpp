@@ -1,6 +1,5 @@
 // ep2d_batch.hpp -- many RVEs on one B200: batched persistent iteration under a CUDA
-// graph (north-star addition 2) and the continuous-batching engine the server uses
-// (addition 3).
+// graph and the continuous-batching engine the server uses.
 //
 // Every RVE runs its own ComputeEffModuli chain (EffPlast2D.cu:179-229): preload time
 // steps, then the load increments, each iterated until the reference's convergence

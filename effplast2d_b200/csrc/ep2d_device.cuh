@@ -51,7 +51,7 @@ __device__ __forceinline__ double host_pos(double h, long n_minus, long idx) {
   return __dadd_rn(__dmul_rn(__dmul_rn(-0.5, h), (double)n_minus), __dmul_rn(h, (double)idx));
 }
 
-// Mask setup (north-star item d): one thread per node.
+// Mask setup: one thread per node.
 __global__ void k_mask(Geo g, uint8_t* __restrict__ mask) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;

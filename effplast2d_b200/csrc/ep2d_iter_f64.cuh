@@ -1,4 +1,4 @@
-// ep2d_iter_f64.cuh -- the fused iteration kernel (north-star items a and b), single
+// ep2d_iter_f64.cuh -- the fused iteration kernel, tile form (stress, return, update), single
 // RVE and batched.
 //
 // One launch = one pseudo-time iteration of the reference's four kernels
@@ -15,7 +15,7 @@
 //   D  damped momentum update and U += V dt on the owned faces, U written to the other
 //      ping-pong buffer.
 // Stresses stay on chip; RECORD launches (checkpoints, last iteration) also write the
-// stress fields and fold max|Vx|, max|Vy| into vmax (north-star item c).
+// stress fields and fold max|Vx|, max|Vy| into vmax (the convergence norm).
 //
 // Arithmetic: displacements and all arithmetic are FP64; velocities are stored as TV
 // (double on the plain path, float on the mixed path: velocities only scale the next

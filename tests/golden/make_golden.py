@@ -11,7 +11,7 @@ builds from the reference's own sources into oracle/_ref/ (`make -C oracle ref`)
                     data/*.dat outputs)
 
 Usage: python tests/golden/make_golden.py [out_dir] [--only name,...] [--with-cfg2]
-Writes <name>.npz (+ .json metadata) per case into out_dir (default gpurun_out/golden).
+Writes <name>.npz (+ .json metadata) per case into out_dir (default golden_out/ at the repository root).
 """
 import json
 import os
@@ -229,7 +229,7 @@ def reduce_fixture(path_in, path_out, stride=8):
 
 def main():
     argv = sys.argv[1:]
-    out = os.path.join(ROOT, "gpurun_out", "golden")
+    out = os.path.join(ROOT, "golden_out")
     only = None
     with_cfg2 = False
     rest = []

@@ -4,8 +4,8 @@
 over two time steps, then the bulk increment (NL = 2), EITER = 1e-9, NITER = 5e6.  The
 reference needs 110,000 + 5,000,000 (capped, not converged) + 1,940,000 iterations.  The
 fixture keeps the reference's records and moduli at 17 digits and every 8th row and
-column of its final fields (tests/golden/make_golden.py reduce_fixture).  Bars: the
-north star's 1e-6 on fields and 1e-5 on the moduli; identical iteration counts.
+column of its final fields (tests/golden/make_golden.py reduce_fixture).  Bars: 1e-6
+on fields and 1e-5 on the moduli; identical iteration counts.
 """
 import json
 import math

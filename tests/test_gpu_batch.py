@@ -2,9 +2,9 @@
 
 Each RVE of a batch must give exactly what the single-RVE path gives for the same
 inputs (every kernel form, batched or not, evaluates the same explicitly rounded
-per-cell formulas, so neither the form, the rows nor the batch changes a bit), the mixed-precision batch must stay within the
-north-star bar of 1e-5 relative on K_phi, K_d and G, and the server must return the
-same result for a request alone and in a mix.
+per-cell formulas, so neither the form, the rows nor the batch changes a bit), the
+mixed-precision batch must stay within the parity bar of 1e-5 relative on K_phi, K_d
+and G, and the server must return the same result for a request alone and in a mix.
 """
 import math
 

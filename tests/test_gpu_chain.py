@@ -4,7 +4,7 @@ The GPU path runs preload, averaging, boundary sums, hole area and moduli on the
 device + host exactly as the reference orders them; the oracle restates the reference
 sequentially.  Sums are reduced in a different order on the GPU (deterministic tree),
 so scalars agree to rounding: tolerance 1e-9 relative on every record value and on the
-moduli (1e-5 on K_d, K_phi, G).
+moduli (the parity bar is 1e-5 on K_d, K_phi, G).
 """
 import math
 
