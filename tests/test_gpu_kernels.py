@@ -131,12 +131,14 @@ def test_homogeneous_affine_is_equilibrium():
     assert np.allclose(P, P[1, 1], rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("grid", [(301, 203), (242, 130)], ids=["301x203", "242x130"])
 @pytest.mark.parametrize("rows", [16, 64, 256])
-def test_stream_form_matches_tile_form(rows):
+def test_stream_form_matches_tile_form(rows, grid):
     # Both forms evaluate the same explicitly rounded per-cell formulas, so they agree
-    # bit for bit.  The grid is wider and taller than several strips and segments,
-    # ragged in both, so interior and edge segments both run.
-    nx, ny = 301, 203
+    # bit for bit.  The grids are wider and taller than several strips and segments,
+    # ragged in both, so interior and edge segments both run; the last strip holds 21
+    # (301) and 18 (242) columns of the grid.
+    nx, ny = grid
     pa = _pa(nx, ny, n_pores=4, porosity=0.03, yield_stress=1e-5)
     st = _random_state(nx, ny, 11)
     out = []
