@@ -19,11 +19,13 @@
 // is carried in a register instead of fetched again.  There is no block-wide barrier;
 // each lane reads only the ring entries it wrote.
 //
-// Segments whose 32 columns and rows jA-3 .. jB+1 lie inside the grid away from its
+// Segments whose 32 columns and rows jA-2 .. jB+1 lie inside the grid away from its
 // edges run the INTERIOR instantiation: no bounds tests, and the clamped 2x2 corner
 // block of the node return is always the one below-left.  Segments touching an edge
 // run the general one.  Both call the same formulas, so they round alike.
 #pragma once
+
+#include <type_traits>
 
 #include "ep2d_stencil.cuh"
 #include "ep2d_types.hpp"
@@ -88,8 +90,8 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // true if segment (strip, jA..jB) may run the INTERIOR instantiation: every lane's
-// column in [0, nx-1] and at least one column from the right edge, rows jA-3 .. jB+1
-// inside the grid with jB <= ny-2
+// column in [0, nx-1] and at least one column from the right edge, rows jA-2 .. jB+1
+// inside the grid with jA >= 3 and jB <= ny-2
 __device__ __forceinline__ bool stream_interior(int nx, int ny, int strip, int jA, int jB) {
   return strip >= 1 && STREAM_COLS * strip + 29 <= nx - 3 && jA >= 3 && jB <= ny - 2;
 }
@@ -123,7 +125,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   // a 16-byte aligned address (pitch % 32 == 0) and lies in its row as long as it starts
   // inside the pitch.  Columns past the grid read the row padding, which nothing writes
   // and which holds zeros, like the zero fill of rows and columns outside the arrays.
-  const int k_first = jA - 3, k_last = jB + 1;
+  const int k_first = jA - 2, k_last = jB + 1;
   const int half = lane >> 4;                                  // 0: Ux, Vx; 1: Uy, Vy
   const int pc = STREAM_COLS * strip - 2 + 2 * (lane & 15);    // first column of the pair
   const bool pair_in = INTERIOR || (pc >= 0 && pc < pitch);
@@ -197,12 +199,13 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     cp_async_commit();
     slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
   };
-  take_row();  // rows k_first and k_first + 1 only fill the registers
-  k++;
-  take_row();
-  k++;
-#pragma unroll 2
-  for (; k <= k_last; k++) {
+  // Step r = k - 1 forms the trial stresses of row r, returns row r - 1 (STAGE >= 1)
+  // and updates the faces of row r - 1 (STAGE 2).  The first owned face row, jA, needs
+  // rows jA and jA - 1 returned, and those need the trials of rows jA - 2 .. jA: the
+  // march opens with two trial-only steps (r = jA - 2, jA - 1) and one without faces
+  // (r = jA), then takes one full step per owned row.
+  auto step = [&](auto stage_c) {
+    constexpr int STAGE = decltype(stage_c)::value;
     take_row();
     const int r = k - 1;
 
@@ -236,52 +239,55 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
 
     // ---- return of row j = r - 1
     const int j = r - 1;
-    double xr = xa, yr = ya, cr = c2;
     double tav_o = 0.0, j2_o = 0.0, j2xy_o = 0.0;
-    if (PLASTIC) {
-      // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
-      double c00, c10, c01, c11;
-      if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j)
-        c00 = c1_l; c10 = c1; c01 = c2_l; c11 = c2;
-      } else {
-        const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
-        const int bsel = min(max(j - 1, 0), ny - 3) - j;
-        const double cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
-        const double cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
-        const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
-        c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
-        c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
+    double cq_l = 0.0;
+    if constexpr (STAGE >= 1) {
+      double xr = xa, yr = ya, cr = c2;
+      if (PLASTIC) {
+        // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
+        double c00, c10, c01, c11;
+        if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j)
+          c00 = c1_l; c10 = c1; c01 = c2_l; c11 = c2;
+        } else {
+          const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
+          const int bsel = min(max(j - 1, 0), ny - 3) - j;
+          const double cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
+          const double cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
+          const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
+          c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
+          c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
+        }
+        const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
+        const double nJ2sq = node_j2sq(xa, ya, tav);
+        const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
+        const double fn = node_in ? return_factor(nJ2sq, coh, coh2) : 1.0;
+        // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
+        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
+        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
+        const double cJ2sq = corner_j2sq(sx, sy, c2);
+        const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
+        const double fc = corner_in ? return_factor(cJ2sq, coh, coh2) : 1.0;
+        if (RECORD) {
+          tav_o = node_in ? __dmul_rn(tav, fn) : 0.0;
+          j2_o = !node_in ? 0.0
+                          : (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o))
+                                        : __dsqrt_rn(nJ2sq);
+          j2xy_o = corner_in ? __dsqrt_rn(cJ2sq) : 0.0;
+        }
+        xr = __dmul_rn(xa, fn);
+        yr = __dmul_rn(ya, fn);
+        cr = __dmul_rn(c2, fc);
       }
-      const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
-      const double nJ2sq = node_j2sq(xa, ya, tav);
-      const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
-      const double fn = node_in ? return_factor(nJ2sq, coh, coh2) : 1.0;
-      // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
-      const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
-      const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
-      const double cJ2sq = corner_j2sq(sx, sy, c2);
-      const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
-      const double fc = corner_in ? return_factor(cJ2sq, coh, coh2) : 1.0;
-      if (RECORD) {
-        tav_o = node_in ? __dmul_rn(tav, fn) : 0.0;
-        j2_o = !node_in ? 0.0
-                        : (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o))
-                                      : __dsqrt_rn(nJ2sq);
-        j2xy_o = corner_in ? __dsqrt_rn(cJ2sq) : 0.0;
-      }
-      xr = __dmul_rn(xa, fn);
-      yr = __dmul_rn(ya, fn);
-      cr = __dmul_rn(c2, fc);
+      cq_l = cw_l;
+      pq = pw; yq = yw; cq = cw;
+      pw = pa_; xw = xr; yw = yr; cw = cr;
+      cw_l = shfl_up1(cw);
     }
-    const double cq_l = cw_l;
-    pq = pw; yq = yw; cq = cw;
-    pw = pa_; xw = xr; yw = yr; cw = cr;
-    cw_l = shfl_up1(cw);
 
     // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring.  A face
     // the reference leaves alone gets its old velocity back, unchanged.
-    const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
-    if (j >= jA) {
+    if constexpr (STAGE == 2) {
+      const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
       const StreamRow<TV>& rj = sm.ring[s_k2];
       const double uxm = rj.ux[lane], uym = rj.uy[lane];
       const double vxm = (double)rj.vx[lane], vym = (double)rj.vy[lane];
@@ -323,7 +329,17 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         }
       }
     }
-  }
+  };
+  take_row();  // row jA - 2 only fills the registers
+  k++;
+  step(std::integral_constant<int, 0>{});
+  k++;
+  step(std::integral_constant<int, 0>{});
+  k++;
+  step(std::integral_constant<int, 1>{});
+  k++;
+#pragma unroll 2
+  for (; k <= k_last; k++) step(std::integral_constant<int, 2>{});
 }
 
 template <bool PLASTIC, bool RECORD, typename TV>
