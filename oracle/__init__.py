@@ -3,7 +3,7 @@
 Python access to liboracle.so (ep2d_oracle.c, the plain-C FP64 restatement of the
 reference's EffPlast2D.cu) and to the reference's own binaries under oracle/_ref.
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module,
-and only as the checker.  The product package never imports it.
+and only to check results or time the CPU baseline.  The product package never imports it.
 """
 import ctypes
 import math

@@ -2,8 +2,8 @@
  * ep2d_oracle.h -- CPU oracle for the EffPlast2D pseudo-transient solver.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference's FP64
- * algorithm (beacon1143/EffPlast2D, EffPlast2D.cu) used as the checker by tests/, by
- * __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  The product
+ * algorithm (beacon1143/EffPlast2D, EffPlast2D.cu) that tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg check results against.  The product
  * (effplast2d_b200, libep2d.so) never links or calls it.
  *
  * The API mirrors include/ep2d.h one to one (orc_* <-> ep2d_*) so that a test can
