@@ -20,7 +20,8 @@ time is the max over ranks; value = work of all ranks / that time ("scaling": "w
 
 --impl reference times the reference algorithm on the host cores (the CPU restatement
 of EffPlast2D.cu, all threads) on a bounded sample of the same workload and converts its
-cell-update rate into solves/s with the same iteration count.  Rank 0 only.
+cell-update rate into solves/s with the same iteration count.  Rank 0 only.  Both
+cpu_baseline objects add a single-thread sample of the same restatement.
 """
 import argparse
 import json
@@ -213,6 +214,7 @@ def run_reference(args, w):
             vals.append(rate)
     rate = statistics.median(vals)
     v = rate / (n * n * total_iters)
+    rate1, _, desc1 = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_1T_S", "4")), threads=1)
     line = {
         "impl": "reference", "metric": "converged RVE solves/s", "value": v, "unit": "RVE solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
@@ -220,7 +222,8 @@ def run_reference(args, w):
         "config": {"workload": args.workload, "description": w["label"], "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
                          "sample": desc + "; solves/s = cell-update rate / (%d^2 cells x %d iterations per solve, "
-                                          "from the reference's own run)" % (n, total_iters)},
+                                          "from the reference's own run)" % (n, total_iters),
+                         "single_thread": {"value": rate1 / (n * n * total_iters), "cores": 1, "sample": desc1}},
         "e2e": {"value": v, "unit": "RVE solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -382,9 +385,11 @@ def run_ours(args, w):
                            "moduli": {"kd": res["num"]["kd"], "kphi": res["num"]["kphi"], "g": res["num"]["g"]}}
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, desc = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_S", "12")))
+            rate1, _, desc1 = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_1T_S", "4")), threads=1)
             v = rate / (n * n * ips)
             line["cpu_baseline"] = {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
-                                    "sample": desc + "; converted with %d iterations per solve" % ips}
+                                    "sample": desc + "; converted with %d iterations per solve" % ips,
+                                    "single_thread": {"value": rate1 / (n * n * ips), "cores": 1, "sample": desc1}}
     if world > 1:
         import torch.distributed as dist
 
