@@ -3,11 +3,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <thread>
 
 namespace ep2d {
@@ -418,6 +420,7 @@ int BatchEngine::run_interval() {
     rc = advance(s, s.rve->error_from_vmax(vmx, vmy));
     if (rc) {
       s.task.status = rc;
+      s.task.error = last_error();
       s.task.done = true;
       s.task.done_s = now_s();
       finished_.push_back(s.task);
@@ -434,6 +437,21 @@ std::vector<Task> BatchEngine::take_finished() {
   std::vector<Task> out;
   out.swap(finished_);
   return out;
+}
+
+void BatchEngine::abort_all(int status, const std::string& error) {
+  for (auto& s : slots_) {
+    if (!s.used) continue;
+    s.task.status = status;
+    s.task.error = error;
+    s.task.done = true;
+    s.task.done_s = now_s();
+    finished_.push_back(s.task);
+    bytes_ -= footprint(s.task.spec);
+    s.rve.reset();
+    s.used = false;
+  }
+  tiles_dirty_ = true;
 }
 
 // ---- server -------------------------------------------------------------------------
@@ -457,33 +475,42 @@ class Server {
   }
   int submit(const ep2d_rve_spec& s, uint64_t* ticket) {
     std::lock_guard<std::mutex> lk(mu_);
-    if (!init_ok_) return fail(EP2D_ERR_STATE, "server is not running");
+    if (!init_ok_)
+      return fail(EP2D_ERR_STATE, stop_msg_.empty() ? "server is not running" : "server stopped: " + stop_msg_);
     Task t;
     t.spec = s;
     t.ticket = ++next_ticket_;
     t.submit_s = now_s();
     pending_.push_back(t);
+    outstanding_.insert(t.ticket);
     submitted_++;
     if (ticket) *ticket = t.ticket;
     cv_.notify_all();
     return EP2D_OK;
   }
+  // A finished request's result is handed out once: the wait that reports *done = 1
+  // releases it, and a later wait on the ticket is an argument error, like a wait on a
+  // ticket this server never issued.
   int wait(uint64_t ticket, int32_t timeout_ms, int32_t* done, ep2d_result* res, double* lat, double* queue) {
     std::unique_lock<std::mutex> lk(mu_);
-    auto ready = [&] { return done_.count(ticket) > 0 || !init_ok_; };
+    if (done) *done = 0;
+    if (!outstanding_.count(ticket)) return fail(EP2D_ERR_ARG, "unknown ticket, or its result was already collected");
+    auto ready = [&] { return done_.count(ticket) > 0 || !init_ok_ || !outstanding_.count(ticket); };
     if (timeout_ms < 0) cv_.wait(lk, ready);
     else cv_.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
     auto it = done_.find(ticket);
     if (it == done_.end()) {
-      if (done) *done = 0;
+      if (!outstanding_.count(ticket)) return fail(EP2D_ERR_ARG, "the result was collected by another wait");
       return init_ok_ ? EP2D_OK : fail(EP2D_ERR_STATE, "server stopped");
     }
+    const Task t = it->second;
+    done_.erase(it);
+    outstanding_.erase(ticket);
     if (done) *done = 1;
-    if (res) *res = it->second.result;
-    if (lat) *lat = it->second.done_s - it->second.submit_s;
-    if (queue) *queue = it->second.admit_s - it->second.submit_s;
-    const int st = it->second.status;
-    return st == EP2D_OK ? EP2D_OK : fail(st, "request failed");
+    if (res) *res = t.result;
+    if (lat) *lat = t.done_s - t.submit_s;
+    if (queue) *queue = t.admit_s - t.submit_s;
+    return t.status == EP2D_OK ? EP2D_OK : fail(t.status, "request failed: " + t.error);
   }
   void stats(int64_t* sub, int64_t* adm, int64_t* fin, int64_t* bytes, ep2d_batch_stats* es) {
     std::lock_guard<std::mutex> lk(mu_);
@@ -505,6 +532,11 @@ class Server {
     }
     cv_.notify_all();
     if (!init_ok_) return;
+    // host-side fault injection for tests: EP2D_SERVER_FAIL_AFTER = k makes the worker treat
+    // its k-th checkpoint interval as failed (status EP2D_ERR_CUDA), without touching the GPU
+    const char* inj = std::getenv("EP2D_SERVER_FAIL_AFTER");
+    const int64_t fail_after = inj ? std::atoll(inj) : 0;
+    int64_t intervals = 0;
     while (true) {
       std::vector<Task> admit;
       {
@@ -527,6 +559,7 @@ class Server {
         std::lock_guard<std::mutex> lk(mu_);
         if (rc) {
           t.status = rc;
+          t.error = last_error();
           t.done = true;
           t.admit_s = t.done_s = now_s();
           done_[t.ticket] = t;
@@ -535,9 +568,16 @@ class Server {
           admitted_++;
         }
       }
+      // An interval that fails leaves the engine's state unknown (a CUDA error may have
+      // ended the context): every active and queued request fails with its status, and
+      // the server stops taking requests.
+      int rc = EP2D_OK;
       if (!eng_.idle()) {
-        const int rc = eng_.run_interval();
-        (void)rc;
+        rc = eng_.run_interval();
+        intervals++;
+        if (rc == EP2D_OK && fail_after > 0 && intervals >= fail_after)
+          rc = fail(EP2D_ERR_CUDA, "injected failure of checkpoint interval " + std::to_string(intervals));
+        if (rc) eng_.abort_all(rc, last_error());
       }
       std::vector<Task> fin = eng_.take_finished();
       {
@@ -546,6 +586,19 @@ class Server {
           done_[t.ticket] = t;
           finished_++;
         }
+        if (rc) {
+          stop_msg_ = last_error();
+          init_ok_ = false;  // no request is accepted from here on
+          for (auto& t : pending_) {
+            t.status = rc;
+            t.error = stop_msg_;
+            t.done = true;
+            t.admit_s = t.done_s = now_s();
+            done_[t.ticket] = t;
+            finished_++;
+          }
+          pending_.clear();
+        }
         bytes_snapshot_ = eng_.bytes_in_use();
         stats_snapshot_.kernel_ms = eng_.kernel_ms;
         stats_snapshot_.launches = eng_.launches;
@@ -553,7 +606,8 @@ class Server {
         stats_snapshot_.cell_updates = eng_.cell_updates;
         eng_.fill_stats(&stats_snapshot_);
       }
-      if (!fin.empty()) cv_.notify_all();
+      if (!fin.empty() || rc) cv_.notify_all();
+      if (rc) break;
     }
     std::lock_guard<std::mutex> lk(mu_);
     init_ok_ = false;
@@ -566,6 +620,8 @@ class Server {
   std::condition_variable cv_;
   std::deque<Task> pending_;
   std::map<uint64_t, Task> done_;
+  std::set<uint64_t> outstanding_;  // issued tickets whose result has not been collected
+  std::string stop_msg_;            // why the worker stopped, if it failed
   uint64_t next_ticket_ = 0;
   int64_t budget_ = 0;
   int max_active_ = 0;

@@ -28,6 +28,7 @@ struct Task {
   bool done = false;
   int status = EP2D_OK;
   ep2d_result result{};
+  std::string error;           // why it failed (status != EP2D_OK)
   uint64_t ticket = 0;
   double submit_s = 0.0, admit_s = 0.0, done_s = 0.0;  // host clock (server latency)
 };
@@ -48,6 +49,8 @@ class BatchEngine {
   bool idle() const { return active() == 0; }
   // finished tasks since the last call (slot memory released)
   std::vector<Task> take_finished();
+  // end every active RVE with `status` (slot memory released); they go to take_finished()
+  void abort_all(int status, const std::string& error);
   size_t footprint(const ep2d_rve_spec& s) const;
   size_t bytes_in_use() const { return bytes_; }
 

@@ -307,12 +307,17 @@ typedef struct ep2d_server ep2d_server;
 /* A worker thread owns one batch engine on `cfg->device`.  Requests are admitted at
  * checkpoint boundaries while the summed footprint of the active RVEs stays within
  * mem_budget_bytes and their number within max_active; admitted RVEs stay resident
- * until they converge. */
+ * until they converge.  If a checkpoint interval fails (a CUDA error), every active and
+ * queued request finishes with that status and the server accepts no more requests
+ * (EP2D_ERR_STATE); destroy it and create a new one. */
 int ep2d_server_create(const ep2d_batch_config* cfg, int64_t mem_budget_bytes, int32_t max_active,
                        ep2d_server** out);
 int ep2d_server_submit(ep2d_server* s, const ep2d_rve_spec* spec, uint64_t* ticket_out);
 /* Wait up to timeout_ms (negative: forever) for the request to finish.  *done = 1 and
- * *result / *latency_s (submit to completion, host clock) are filled when it has. */
+ * *result / *latency_s (submit to completion, host clock) / *queue_s are filled when it
+ * has, and the return value is the request's own status.  That wait releases the result:
+ * a later wait on the same ticket, like one on a ticket this server never issued,
+ * returns EP2D_ERR_ARG at once. */
 int ep2d_server_wait(ep2d_server* s, uint64_t ticket, int32_t timeout_ms, int32_t* done,
                      ep2d_result* result, double* latency_s, double* queue_s);
 /* requests submitted, admitted, finished; bytes of device memory in use */

@@ -121,3 +121,36 @@ def test_server_admission_by_memory_budget():
     assert max(o[2] for o in outs) > 0.0
     for sp, o in zip(SPECS[:4], outs):
         check_result(o[0], single(sp), 0.0, sp[4])
+
+
+def test_server_ticket_results_are_collected_once():
+    # the wait that reports a result releases it; waits on that ticket again, or on a
+    # ticket the server never issued, are argument errors (they do not block)
+    with B.Server(mem_budget_bytes=1 << 34, niter=NITER, eiter=1e-9, check_every=CE, kernel=ep.KERNEL_STREAM,
+                  rows=64) as srv:
+        t = srv.submit(mk(*SPECS[0]))
+        assert srv.wait(t, timeout_ms=600000) is not None
+        for bad in (t, t + 1000):
+            with pytest.raises(ep.EP2DError) as ei:
+                srv.wait(bad)
+            assert ei.value.status == ep.ERR_ARG
+
+
+def test_server_fails_every_request_after_an_engine_error(monkeypatch):
+    # host-side fault injection: the worker treats its second checkpoint interval as a
+    # failed CUDA call; every admitted and queued request ends with that status (none can
+    # converge in 2 x 500 iterations), waits return at once, and submissions are refused
+    monkeypatch.setenv("EP2D_SERVER_FAIL_AFTER", "2")
+    specs = [mk(*s) for s in SPECS]
+    with B.Server(mem_budget_bytes=2 * B.footprint(specs[1]), niter=NITER, eiter=1e-9, check_every=CE,
+                  kernel=ep.KERNEL_STREAM, rows=64) as srv:
+        tickets = [srv.submit(s) for s in specs]
+        for t in tickets:
+            with pytest.raises(ep.EP2DError) as ei:
+                srv.wait(t, timeout_ms=600000)
+            assert ei.value.status == ep.ERR_CUDA and "injected" in str(ei.value), str(ei.value)
+        st = srv.stats()
+        assert st["finished"] == len(specs) and st["bytes_in_use"] == 0
+        with pytest.raises(ep.EP2DError) as ei:
+            srv.submit(specs[0])
+        assert ei.value.status == ep.ERR_STATE
