@@ -91,8 +91,8 @@ def test_solver_without_device_fails_loudly():
     assert e.value.status == _abi.ERR_NODEV
 
 
-@pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "zero_pores", "kernel3", "tile_rows12", "stream_rows8",
-                                 "stream_rows2048"])
+@pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "side65537", "field_2e31", "zero_pores", "kernel3",
+                                 "tile_rows12", "stream_rows8", "stream_rows2048"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
     pa = ep.make_pa(20.0, 20.0, 32, 32)
@@ -108,6 +108,10 @@ def test_invalid_params_rejected_before_device(bad):
         nl = 0
     elif bad == "tiny":
         nx = 4
+    elif bad == "side65537":  # more than 65536 nodes per side
+        nx = 65537
+    elif bad == "field_2e31":  # pitch 46,368 x 46,342 rows per field: over the 2^31 index range
+        nx = 46341
     elif bad == "zero_pores":
         pa[10] = 0.0
     with pytest.raises(ep.EP2DError) as e:
