@@ -484,20 +484,29 @@ def run_batch(args):
         res_s.append(s.compute_eff_moduli(r["load"], r["lt"], 1))
         s.close()
     t_single = time.perf_counter() - t
+    # The moduli error is a property of converged solves: an RVE whose time step stops at
+    # NITER in either run compares two unconverged states, whose difference is set by the
+    # residual left, not by the precision.  Both are reported, separately.
     errs = {k: [] for k in ("kphi", "kd", "g")}
+    errs_capped = {k: [] for k in ("kphi", "kd", "g")}
+    n_conv = 0
     for rb, rs, r in zip(res_b, res_s, reqs):
+        both = bool(rb["all_converged"]) and bool(rs["all_converged"])
+        n_conv += both
         for k in errs:
             if k == "g" and r["nl"] < 3:
                 continue
             a, b = rb["num"][k], rs["num"][k]
             if np.isfinite(b) and b != 0:
-                errs[k].append(abs(a - b) / abs(b))
+                (errs if both else errs_capped)[k].append(abs(a - b) / abs(b))
     cells = sum(r["n"] ** 2 * rs["total_iterations"] for r, rs in zip(reqs, res_s))
     print(json.dumps({
         "workload": "batch", "rves": len(reqs), "seed": args.seed, "precision": "mixed (FP32 velocities)",
         "batched_solves_per_s": len(reqs) / t_batch, "single_fp64_solves_per_s": len(reqs) / t_single,
         "speedup": t_single / t_batch, "batched_cell_updates_per_s": cells / t_batch,
+        "converged_rves": n_conv,
         "max_rel_moduli_error": {k: (max(v) if v else None) for k, v in errs.items()},
+        "max_rel_moduli_error_capped": {k: (max(v) if v else None) for k, v in errs_capped.items()},
         "kernel": st["kernel"], "rows": st["rows"], "tune_us": st["tune_us"], "blocks": st["blocks"],
         "sides": sorted({r["n"] for r in reqs})}))
     return 0
@@ -538,8 +547,9 @@ def run_precision(args):
 
 
 def run_serve(args):
-    """Poisson stream of requests into the continuous-batching server: p50/p99 latency
-    and solves/s, with the plain FP64 one-at-a-time path's solves/s beside them."""
+    """Poisson stream of requests into the continuous-batching server: p50/p99 latency,
+    queue time and solves/s (the plain FP64 one-at-a-time path on the same distribution
+    is the batch workload's single-RVE leg)."""
     import numpy as np
 
     import effplast2d_b200 as ep
@@ -565,7 +575,8 @@ def run_serve(args):
         "precision": "mixed (FP32 velocities)", "solves_per_s": len(reqs) / wall,
         "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
         "queue_p50_s": float(np.percentile([o[2] for o in outs], 50)),
-        "all_converged": all(o[0]["all_converged"] for o in outs), "engine": st["engine"]}))
+        "all_converged": all(o[0]["all_converged"] for o in outs),
+        "converged_requests": sum(1 for o in outs if o[0]["all_converged"]), "engine": st["engine"]}))
     return 0
 
 
