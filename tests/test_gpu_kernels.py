@@ -152,3 +152,29 @@ def test_stream_form_matches_tile_form(rows, grid):
     for f in FIELDS + PLASTIC_FIELDS:
         assert np.array_equal(out[1][f], out[0][f]), (f, float(np.max(np.abs(out[1][f] - out[0][f]))))
 
+
+def test_full_size_2048_against_oracle_and_tile_form(rel):
+    # The 2048^2 grid of the 4x4-pore, porosity-0.02, Y = 1e-5 workload at full size: the
+    # library's default shape there (stream form, 64-row segments: one wave of 2368 warps,
+    # interior and edge segments), 20 iterations from a seeded state that yields widely,
+    # bit for bit against the tile form and to 1e-9 against the oracle.
+    n = 2048
+    pa = _pa(n, n, n_pores=4, porosity=0.02, yield_stress=1e-5)
+    st = _random_state(n, n, 5)
+    g = ep.Solver(n, n, pa, nl=3)
+    assert g.kernel_shape() == (ep.KERNEL_STREAM, 64)
+    t = ep.Solver(n, n, pa, nl=3, kernel=ep.KERNEL_TILE, rows=16)
+    o = oracle.Oracle(n, n, pa, nl=3)
+    for k, v in st.items():
+        g.set(k, v)
+        t.set(k, v)
+        o.set(k, v)
+    for it in (1, 19):
+        g.iterate(it)
+        t.iterate(it)
+        o.iterate(it)
+    assert (o.get("J2XY") > pa[8]).mean() > 0.05  # the return map is exercised
+    for f in FIELDS + PLASTIC_FIELDS:
+        a = g.get(f)
+        assert np.array_equal(a, t.get(f)), f
+        assert rel(a, o.get(f)) < 1e-9, f
