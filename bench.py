@@ -19,9 +19,10 @@ Multi-GPU (torchrun, one rank per GPU): every rank iterates / solves its own RVE
 time is the max over ranks; value = work of all ranks / that time ("scaling": "weak").
 
 --impl reference times the reference algorithm on the host cores (the CPU restatement
-of EffPlast2D.cu, all threads) on a bounded sample of the same workload and converts its
-cell-update rate into solves/s with the same iteration count.  Rank 0 only.  Both
-cpu_baseline objects add a single-thread sample of the same restatement.
+of EffPlast2D.cu's four kernels, all threads): each step is the same 10,000-iteration
+step of the same preloaded RVE, host-timed, and solves/s uses the same iteration count.
+Rank 0 only.  Both cpu_baseline objects add a single-thread sample of the same
+restatement.  Both arms print the same `config` object.
 """
 import argparse
 import json
@@ -164,7 +165,7 @@ def cpu_sample(w, seconds=12.0, threads=None):
     workload's preloaded state: returns (cell updates per second, threads, description)."""
     import oracle
 
-    threads = threads or os.cpu_count() or 1
+    threads = threads or host_threads()
     oracle.set_threads(threads)
     n = w["n"]
     pa = make_pa_oracle(w)
@@ -193,38 +194,78 @@ def make_pa_oracle(w):
                           n_pores=w["n_pores"])
 
 
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def bench_config(w, workload, world, ips):
+    """The `config` object both arms print: it names the workload and the step, nothing
+    about the implementation that runs it, so the two arms' objects are equal."""
+    return {"workload": workload, "description": w["label"],
+            "step": "%d pseudo-time iterations (one checkpoint interval) of the preloaded RVE" % w["check_every"],
+            "iterations_per_solve": ips,
+            "value_from": "solves/s = iterations/s / iterations_per_solve (recorded from the reference's own run of "
+                          "this workload and reproduced exactly by this implementation)",
+            "global_batch": world,
+            "l2": "device arm: a 256 MB buffer is written between timed steps (the %d^2 state, %.0f MB, is "
+                  "L2-resident within a step); host arm: no device" % (w["n"], 13 * 8 * w["n"] ** 2 / 1e6),
+            "parallelism": "replicas x%d" % world}
+
+
 def run_reference(args, w):
+    """The reference algorithm on the host cores: the CPU restatement of EffPlast2D.cu's
+    four kernels (oracle, OpenMP over all host threads), one step = the same
+    check_every-iteration step of the same preloaded RVE as the device arm, timed with
+    the host clock.  Warm-up steps are shorter (200 iterations): they only warm the
+    caches and the thread pool."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    p = os.path.join(ROOT, "tests", "golden", args.workload + ".json")
-    if not os.path.exists(p):
+    ips = iterations_per_solve(args.workload)
+    if not ips:
         print(json.dumps({"impl": "reference", "unavailable": "no recorded reference run of workload %s" % args.workload}))
         return 0
-    meta = json.load(open(p))
-    total_iters = meta.get("total_iterations")
+    import oracle
+
     n = w["n"]
-    secs = float(os.environ.get("EP2D_REF_SAMPLE_S", "8"))
-    vals = []
-    desc = ""
-    threads = os.cpu_count() or 1
-    for k in range(args.warmup + args.steps):
-        rate, threads, desc = cpu_sample(w, seconds=secs if k >= args.warmup else 1.0)
-        if k >= args.warmup:
-            vals.append(rate)
-    rate = statistics.median(vals)
-    v = rate / (n * n * total_iters)
+    step_iters = int(os.environ.get("EP2D_REF_STEP_ITERS", str(w["check_every"])))
+    threads = host_threads()
+    oracle.set_threads(threads)
+    o = oracle.Oracle(n, n, make_pa_oracle(w), nl=w["nl"], niter=1, eiter=w["eiter"], check_every=w["check_every"])
+    ux, uy = preloaded_state(w)
+    o.set("Ux", ux)
+    o.set("Uy", uy)
+    for _ in range(args.warmup):
+        o.iterate(200)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        o.iterate(step_iters)
+        times.append(time.perf_counter() - t)
+    o.close()
+    total = sum(times)
+    iters_per_s = args.steps * step_iters / total
+    v = iters_per_s / ips
     rate1, _, desc1 = cpu_sample(w, seconds=float(os.environ.get("EP2D_CPU_SAMPLE_1T_S", "4")), threads=1)
+    desc = ("%d steps of %d pseudo-time iterations of the %dx%d preloaded state on %d host threads (%.1f s); "
+            "solves/s = iterations/s / %d iterations per solve (the reference's own run)"
+            % (args.steps, step_iters, n, n, threads, total, ips))
     line = {
         "impl": "reference", "metric": "converged RVE solves/s", "value": v, "unit": "RVE solves/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": w["label"], "parallelism": "host threads"},
-        "cpu_baseline": {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
-                         "sample": desc + "; solves/s = cell-update rate / (%d^2 cells x %d iterations per solve, "
-                                          "from the reference's own run)" % (n, total_iters),
-                         "single_thread": {"value": rate1 / (n * n * total_iters), "cores": 1, "sample": desc1}},
-        "e2e": {"value": v, "unit": "RVE solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": bench_config(w, args.workload, world, ips),
+        "implementation": "CPU restatement of EffPlast2D.cu's four kernels (ComputeStress, ComputeJ2, "
+                          "ComputePlasticity, ComputeDisp), unfused as the reference runs them, FP64",
+        "cpu_baseline": {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port", "sample": desc,
+                         "single_thread": {"value": rate1 / (n * n * ips), "cores": 1, "sample": desc1}},
+        # the host arm has no host<->device traffic: its end-to-end rate is its rate
+        "e2e": {"value": v, "unit": "RVE solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "step": "the same host step as value (no device, nothing to copy)"},
+        "cell_updates_per_s": iters_per_s * n * n,
     }
     print(json.dumps(line))
     return 0
@@ -357,15 +398,8 @@ def run_ours(args, w):
             "metric": "converged RVE solves/s", "value": value, "unit": "RVE solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "description": w["label"],
-                       "step": "%d pseudo-time iterations (one checkpoint interval) of the preloaded RVE" % step_iters,
-                       "iterations_per_solve": ips,
-                       "value_from": "solves/s = iterations/s / iterations_per_solve (recorded from the reference's "
-                                     "own run of this workload and reproduced exactly by this implementation)",
-                       "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
-                       "global_batch": world, "l2": "256 MB buffer written between steps (the %d^2 state, %.0f MB, "
-                       "is L2-resident within a step)" % (n, 13 * 8 * n * n / 1e6),
-                       "parallelism": "replicas x%d" % world},
+            "config": bench_config(w, args.workload, world, ips),
+            "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
             "e2e": None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(args.workload),

@@ -12,9 +12,15 @@
 // it (kMaxBlocks x NAVG doubles, 176 KiB) until the process exits.  Host code must not
 // use its name as an address -- on the host the name is only a stand-in -- so the first
 // call on each device looks its device address up with cudaGetSymbolAddress while that
-// device is current, and passes that pointer to the kernels.  Every call overwrites all
-// the partials it later reads, so nothing needs clearing between calls; calls that
-// overlap on the GPU would share the array and race.
+// device is current, and passes that pointer to the kernels.  The address belongs to the
+// device's current context: after a cudaDeviceReset the module is loaded again, possibly
+// elsewhere, so the lookup is keyed on the context too and the first call in a new
+// context repeats it.  That first call (per device, and again after a reset) should come
+// before any stream capture.  Every call overwrites all the partials it later reads, so
+// nothing needs clearing between calls; calls that overlap on the GPU would share the
+// array and race.
+#include <cuda.h>
+
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -34,21 +40,45 @@ static __device__ __align__(256) double g_avg_scratch[kMaxBlocks * NAVG];
 
 std::mutex g_scratch_mu;
 double* g_scratch_dev[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};  // the context each cached address belongs to
 
-// The scratch array's device address on the current device, looked up once per device.
+// cuCtxGetCurrent through the runtime's driver entry point (no link against libcuda)
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// The scratch array's device address on the current device, looked up once per device
+// and context.
 int scratch_on_current_device(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(EP2D_ERR_NODEV, std::string("no current CUDA device: ") + cudaGetErrorString(e));
+  // cudaFree(nullptr) makes the device's primary context current without allocating
+  e = cudaFree(nullptr);
+  CUcontext ctx = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (e != cudaSuccess || !get || get(&ctx) != CUDA_SUCCESS || !ctx)
+    return fail(EP2D_ERR_CUDA, std::string("no current CUDA context for the scratch lookup: ") +
+                                   cudaGetErrorString(e));
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
+  if (!g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_avg_scratch);
     if (e != cudaSuccess || !p)
       return fail(EP2D_ERR_CUDA, std::string("cudaGetSymbolAddress of the averaging scratch: ") +
                                      cudaGetErrorString(e));
     g_scratch_dev[dev] = static_cast<double*>(p);
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_dev[dev];
   return EP2D_OK;
@@ -135,9 +165,17 @@ extern "C" int ep2d_average_fields_noalloc(int32_t nx, int32_t ny, const double 
     return fail(EP2D_ERR_ARG, "ny = " + std::to_string(ny) + " exceeds " +
                                   std::to_string(ep2d::kMaxBlocks * ep2d::kRowsPerBlock + 2) +
                                   ", the largest grid the scratch-free averaging supports");
+  // the checks of the library's parameter validation that concern the averaging
   for (int k = 0; k < EP2D_NPARS; k++)
     if (!std::isfinite(pa[k])) return fail(EP2D_ERR_ARG, "pa[" + std::to_string(k) + "] is not finite");
-  if (!(pa[10] >= 1.0)) return fail(EP2D_ERR_ARG, "N (pores per side) must be >= 1");
+  if (!(pa[0] > 0.0) || !(pa[1] > 0.0)) return fail(EP2D_ERR_ARG, "dX and dY must be positive");
+  if (!(pa[10] >= 1.0) || pa[10] > 64.0) return fail(EP2D_ERR_ARG, "N (pores per side) must be in [1, 64]");
+  if (!(3.0 * pa[3] + pa[4] != 0.0)) return fail(EP2D_ERR_ARG, "3 K0 + G0 must not be zero");
+  // an error left by the caller's earlier work is reported as such, not as this call's
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return fail(EP2D_ERR_CUDA, std::string("a CUDA error from earlier work is pending (nothing launched): ") +
+                                   cudaGetErrorString(pending));
   double* scratch = nullptr;
   const int rc = ep2d::scratch_on_current_device(&scratch);
   if (rc) return rc;

@@ -338,9 +338,12 @@ int ep2d_server_destroy(ep2d_server* s);
  *   divided as the reference divides them (the values ep2d_step_record holds).
  * The reduction's partial sums use a fixed device array of 2048 x 11 doubles (176 KiB,
  * held by every GPU that loads the library until the process exits), so ny may be at
- * most 8194; a larger ny returns EP2D_ERR_ARG without touching the GPU.  The first call
- * on a device looks the array's address up (cudaGetSymbolAddress) with that device
- * current: make that first call before any stream capture.  All calls share the array,
+ * most 8194; a larger ny returns EP2D_ERR_ARG without touching the GPU, as do dX or dY
+ * not positive and N outside [1, 64].  A CUDA error left pending by earlier work is
+ * reported (EP2D_ERR_CUDA) and nothing is launched.  The first call on a device looks
+ * the array's address up (cudaGetSymbolAddress) with that device current, and again
+ * after a cudaDeviceReset (the lookup is kept per device and context): make that first
+ * call before any stream capture.  All calls share the array,
  * so calls that overlap on the GPU race: issue them on one stream.  The work is queued
  * on `stream` (a cudaStream_t; NULL: the default stream) and the call returns without
  * waiting for it. */

@@ -109,8 +109,8 @@ def test_dropin_cli_vs_reference(name):
 
 
 def test_dropin_unity_build_vs_reference():
-    # the self-contained build INTEGRATION.md gives (library sources compiled into the
-    # binary with -DEP2D_UNITY): same log and .dat files as the reference's
+    # the self-contained build (library sources compiled into the drop-in binary with
+    # -DEP2D_UNITY, no separate libep2d.so): same log and .dat files as the reference's
     name = "c64_nl2"
     meta, z = load(name)
     exe = epbuild.build_cli_unity(meta["macros"] | {"NPARS": 11, "DEVICE_IDX": 0},
