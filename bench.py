@@ -424,6 +424,16 @@ def run_ours(args, w):
             line["cpu_baseline"] = {"value": v, "unit": "RVE solves/s", "cores": threads, "kind": "port",
                                     "sample": desc + "; converted with %d iterations per solve" % ips,
                                     "single_thread": {"value": rate1 / (n * n * ips), "cores": 1, "sample": desc1}}
+        if world == 1 and not args.no_extras:
+            # the HBM-bound case of the same kernel (the 1024^2 state above is L2-resident)
+            line["roofline_hbm"] = dict(kernel_timing("cfg3", args.hbm_iters),
+                                        note="2048x2048 grid, FP64: 13 fields of 34 MB (0.45 GB) > 126 MB L2; "
+                                             "achieved = 64 B x 2048^2 per launch / CUDA-event time per launch; "
+                                             "traffic from the committed ncu capture of this kernel and grid")
+            # the metric's batched and served headline, sized to fit this run
+            line["batched"] = batch_object(args.extra_batch, args.seed, args.extra_niter)
+            line["served"] = serve_object(args.extra_requests, args.seed, args.rate, args.extra_niter,
+                                          sides=(256, 512, 768, 1024))
     if world > 1:
         import torch.distributed as dist
 
@@ -434,35 +444,50 @@ def run_ours(args, w):
     return 0
 
 
-def run_kernel_only(args, w):
-    """Exactly N pseudo-time iterations of the workload's preload step (no convergence
-    test): the fixed, short launch sequence used for ncu captures and for timing the
-    fused iteration kernel alone."""
+def kernel_timing(workload, iters, kernel=0, rows=0, precision="fp64"):
+    """Exactly `iters` pseudo-time iterations of the workload's preload step (no
+    convergence test), after one untimed pass of the same length: CUDA-event time per
+    launch of the fused iteration kernel on its own stream, and its HBM roofline.
+    precision "f32": the FP32 bulk's FP32 form (32 B per cell-update: u' and V in FP32)."""
     import torch
 
     import effplast2d_b200 as ep
 
+    w = WORKLOADS[workload]
     n = w["n"]
-    iters = args.kernel_only
+    prec = {"fp64": ep.FP64, "mixed": ep.MIXED, "f32": ep.F32_BULK}[precision]
     s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=iters, eiter=0.0, check_every=iters, device=0,
-                  kernel=args.kernel, rows=args.rows)
+                  kernel=kernel, rows=rows, precision=prec)
     s.solve_step(0, w["load"], list(w["load_type"]), 1)  # warm-up and preload
+    if precision == "f32":
+        s.iterate_f32(iters)
     st0 = s.stats()
     torch.cuda.synchronize()
     t = time.perf_counter()
-    s.solve_step(0, w["load"], list(w["load_type"]), 1)
+    if precision == "f32":
+        s.iterate_f32(iters)
+    else:
+        s.solve_step(0, w["load"], list(w["load_type"]), 1)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t
     st1 = s.stats()
-    per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(st1["launches"] - st0["launches"], 1)
-    bytes_alg = 64 * n * n
-    peak, kind = measured_peaks()
-    print(json.dumps({"workload": args.workload, "kernel": args.kernel, "rows": args.rows,
-                      "iterations": iters, "avg_launch_us": per * 1e3,
-                      "achieved_gbs": bytes_alg / (per / 1e3) / 1e9, "peak_gbs": peak, "peak_source": kind,
-                      "frac": bytes_alg / (per / 1e3) / 1e9 / peak, "wall_s": wall,
-                      "cell_updates_per_s": n * n / (per / 1e3)}))
+    shape = s.kernel_shape()
     s.close()
+    per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(st1["launches"] - st0["launches"], 1)
+    bytes_alg = {"fp64": 64, "mixed": 48, "f32": 32}[precision] * n * n
+    peak, kind = measured_peaks()
+    achieved = bytes_alg / (per / 1e3) / 1e9
+    return {"workload": workload, "grid": "%dx%d" % (n, n), "iterations": iters, "precision": precision,
+            "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
+            "avg_launch_us": per * 1e3, "algorithmic_bytes_per_launch": bytes_alg, "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "peak_source": kind, "frac": achieved / peak,
+            "traffic": ncu_traffic(workload), "wall_s": wall, "cell_updates_per_s": n * n / (per / 1e3)}
+
+
+def run_kernel_only(args, w):
+    """The fixed, short launch sequence used for ncu captures and for timing the fused
+    iteration kernel alone."""
+    print(json.dumps(kernel_timing(args.workload, args.kernel_only, args.kernel, args.rows, args.precision)))
     return 0
 
 
@@ -495,17 +520,18 @@ def sample_requests(count, seed, sides=(256, 512, 768, 1024)):
     return out
 
 
-def run_batch(args):
-    """Batched mixed-precision solve of a seeded set of RVEs against the plain FP64
-    single-RVE path solving the same RVEs one at a time."""
+def batch_object(count, seed, niter, sides=(256, 512, 768, 1024)):
+    """Batched mixed-precision solve of `count` seeded RVEs of the batched workload's
+    distribution against the plain FP64 single-RVE path solving the same RVEs one at a
+    time (host wall clock around each leg, device work included)."""
     import numpy as np
     import torch
 
     import effplast2d_b200 as ep
     from effplast2d_b200 import batch as B
 
-    reqs = sample_requests(args.batch_size, args.seed)
-    niter = args.niter
+    reqs = sample_requests(count, seed, sides=sides)
+    torch.cuda.synchronize()
     t = time.perf_counter()
     res_b, st = B.batch_solve([r["spec"] for r in reqs], niter=niter, eiter=1e-9, check_every=10_000,
                               precision=ep.MIXED)
@@ -524,9 +550,11 @@ def run_batch(args):
     errs = {k: [] for k in ("kphi", "kd", "g")}
     errs_capped = {k: [] for k in ("kphi", "kd", "g")}
     n_conv = 0
+    same_iters = True
     for rb, rs, r in zip(res_b, res_s, reqs):
         both = bool(rb["all_converged"]) and bool(rs["all_converged"])
         n_conv += both
+        same_iters &= rb["total_iterations"] == rs["total_iterations"]
         for k in errs:
             if k == "g" and r["nl"] < 3:
                 continue
@@ -534,22 +562,32 @@ def run_batch(args):
             if np.isfinite(b) and b != 0:
                 (errs if both else errs_capped)[k].append(abs(a - b) / abs(b))
     cells = sum(r["n"] ** 2 * rs["total_iterations"] for r, rs in zip(reqs, res_s))
-    print(json.dumps({
-        "workload": "batch", "rves": len(reqs), "seed": args.seed, "precision": "mixed (FP32 velocities)",
+    return {
+        "rves": len(reqs), "seed": seed, "sides": sorted({r["n"] for r in reqs}),
+        "distribution": "grid side uniform in %s, nPores U{1..4}, porosity U(0.005, 0.05), Y log-uniform "
+                        "[5e-6, 5e-5], preload U(2e-5, 8e-5) along a random unit load type (|xy| <= 0.5), "
+                        "NL U{2, 3}, one time step" % (list(sides),),
+        "niter": niter, "precision": "mixed (FP32 velocities, FP64 stencil arithmetic and reductions)",
         "batched_solves_per_s": len(reqs) / t_batch, "single_fp64_solves_per_s": len(reqs) / t_single,
-        "speedup": t_single / t_batch, "batched_cell_updates_per_s": cells / t_batch,
-        "converged_rves": n_conv,
+        "speedup": t_single / t_batch, "batched_s": t_batch, "single_fp64_s": t_single,
+        "batched_cell_updates_per_s": cells / t_batch, "single_cell_updates_per_s": cells / t_single,
+        "converged_rves": n_conv, "same_iteration_counts": bool(same_iters),
         "max_rel_moduli_error": {k: (max(v) if v else None) for k, v in errs.items()},
         "max_rel_moduli_error_capped": {k: (max(v) if v else None) for k, v in errs_capped.items()},
-        "kernel": st["kernel"], "rows": st["rows"], "tune_us": st["tune_us"], "blocks": st["blocks"],
-        "sides": sorted({r["n"] for r in reqs})}))
+        "kernel": st["kernel"], "rows": st["rows"], "tunes": st["n_tunes"], "solo_intervals": st["solo_intervals"],
+        "blocks": st["blocks"]}
+
+
+def run_batch(args):
+    print(json.dumps(dict(workload="batch", **batch_object(args.batch_size, args.seed, args.niter))))
     return 0
 
 
 def run_precision(args):
-    """The mixed-precision path (FP32 velocity storage) against the plain FP64 path on one
-    workload, both solved to convergence through the whole ComputeEffModuli chain: the
-    relative error of every modulus, iteration counts and solve times."""
+    """The mixed path (FP32 velocity storage) and the FP32 bulk (FP32 stencil until its
+    residual stalls, then FP64) against the plain FP64 path on one workload, each solved to
+    convergence through the whole ComputeEffModuli chain: the relative error of every
+    modulus, iteration counts (FP32 ones included), solve times."""
     import math
 
     import effplast2d_b200 as ep
@@ -558,41 +596,52 @@ def run_precision(args):
     n = w["n"]
     pa = make_pa(w)
     out = {}
-    for name, prec in (("fp64", ep.FP64), ("mixed", ep.MIXED)):
+    runs = (("fp64", ep.FP64), ("mixed", ep.MIXED), ("f32_bulk", ep.F32_BULK))
+    wanted = args.precisions.split(",")
+    for name, prec in runs:
+        if name not in wanted and name != "fp64":
+            continue
         s = ep.Solver(n, n, pa, nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
                       precision=prec)
         t = time.perf_counter()
         res = s.compute_eff_moduli(w["load"], list(w["load_type"]), w["n_time_steps"])
+        st = s.stats()
         out[name] = {"seconds": time.perf_counter() - t, "total_iterations": res["total_iterations"],
+                     "f32_iterations": st["f32_iterations"],
                      "all_converged": bool(res["all_converged"]), "num": res["num"], "num_per": res["num_per"],
-                     "kernel_us": 1000 * s.stats()["kernel_ms"] / max(s.stats()["launches"], 1)}
+                     "kernel_us": 1000 * st["kernel_ms"] / max(st["launches"], 1),
+                     "checks": [s.check_errors(k, t_) for k in range(w["nl"])
+                                for t_ in range(w["n_time_steps"] if k == 0 else 1)]}
         s.close()
     err = {}
-    for kind in ("num", "num_per"):
-        for k in ("kphi", "kd", "g"):
-            a, b = out["mixed"][kind][k], out["fp64"][kind][k]
-            if math.isfinite(a) and math.isfinite(b) and b != 0.0:
-                err["%s_%s" % (kind, k)] = abs(a - b) / abs(b)
-            else:
-                err["%s_%s" % (kind, k)] = None  # undefined in both (e.g. G without shear)
+    for name in out:
+        if name == "fp64":
+            continue
+        e = {}
+        for kind in ("num", "num_per"):
+            for k in ("kphi", "kd", "g"):
+                a, b = out[name][kind][k], out["fp64"][kind][k]
+                if math.isfinite(a) and math.isfinite(b) and b != 0.0:
+                    e["%s_%s" % (kind, k)] = abs(a - b) / abs(b)
+                else:
+                    e["%s_%s" % (kind, k)] = None  # undefined in both (e.g. G without shear)
+        err[name] = e
     print(json.dumps({"workload": "precision", "config": args.precision_workload, "description": w["label"],
-                      "relative_error_mixed_vs_fp64": err, "runs": out}))
+                      "relative_error_vs_fp64": err, "runs": out}))
     return 0
 
 
-def run_serve(args):
-    """Poisson stream of requests into the continuous-batching server: p50/p99 latency,
-    queue time and solves/s (the plain FP64 one-at-a-time path on the same distribution
-    is the batch workload's single-RVE leg)."""
+def serve_object(count, seed, rate, niter, sides=(256, 512, 768, 1024, 2048)):
+    """Poisson stream of `count` requests at `rate`/s into the continuous-batching server
+    (mixed precision, 180 GB admission budget): p50/p99 latency, queue time, solves/s."""
     import numpy as np
 
     import effplast2d_b200 as ep
     from effplast2d_b200 import batch as B
 
-    reqs = sample_requests(args.batch_size, args.seed, sides=(256, 512, 768, 1024, 2048))
-    rng = np.random.default_rng(args.seed + 1)
-    gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
-    niter = args.niter
+    reqs = sample_requests(count, seed, sides=sides)
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
     with B.Server(mem_budget_bytes=int(180e9), niter=niter, eiter=1e-9, check_every=10_000,
                   precision=ep.MIXED) as srv:
         t0 = time.perf_counter()
@@ -604,13 +653,18 @@ def run_serve(args):
         wall = time.perf_counter() - t0
         st = srv.stats()
     lat = np.array([o[1] for o in outs])
-    print(json.dumps({
-        "workload": "serve", "requests": len(reqs), "rate_per_s": args.rate, "seed": args.seed,
-        "precision": "mixed (FP32 velocities)", "solves_per_s": len(reqs) / wall,
+    return {
+        "requests": len(reqs), "rate_per_s": rate, "seed": seed, "sides": sorted({r["n"] for r in reqs}),
+        "niter": niter, "admission_budget_bytes": int(180e9),
+        "precision": "mixed (FP32 velocities, FP64 stencil arithmetic and reductions)",
+        "solves_per_s": len(reqs) / wall, "wall_s": wall,
         "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
         "queue_p50_s": float(np.percentile([o[2] for o in outs], 50)),
-        "all_converged": all(o[0]["all_converged"] for o in outs),
-        "converged_requests": sum(1 for o in outs if o[0]["all_converged"]), "engine": st["engine"]}))
+        "converged_requests": sum(1 for o in outs if o[0]["all_converged"]), "engine": st["engine"]}
+
+
+def run_serve(args):
+    print(json.dumps(dict(workload="serve", **serve_object(args.batch_size, args.seed, args.rate, args.niter))))
     return 0
 
 
@@ -618,7 +672,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch-size", type=int, default=32, help="RVEs of the batch / serve workloads")
     ap.add_argument("--seed", type=int, default=2026)
-    ap.add_argument("--rate", type=float, default=2.0, help="request rate of the serve workload (1/s)")
+    ap.add_argument("--rate", type=float, default=1.0, help="request rate of the serve workload (1/s)")
     ap.add_argument("--niter", type=int, default=2_000_000, help="NITER of the batch / serve workloads")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
                     help="run N iterations of the workload's preload step and report the kernel timing")
@@ -629,10 +683,20 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve", "precision"])
+    ap.add_argument("--precisions", default="mixed,f32_bulk",
+                    help="paths --workload precision compares with FP64 (mixed, f32_bulk)")
     ap.add_argument("--precision-workload", default="cfg3", choices=sorted(WORKLOADS),
                     help="workload of --workload precision (mixed vs FP64 moduli)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "f32"],
+                    help="arithmetic of --kernel-only (f32: the FP32 bulk's FP32 form)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave the batched, served and roofline_hbm objects out of the default line")
+    ap.add_argument("--extra-batch", type=int, default=8, help="RVEs of the default line's batched object")
+    ap.add_argument("--extra-requests", type=int, default=12, help="requests of the default line's served object")
+    ap.add_argument("--extra-niter", type=int, default=2_000_000, help="NITER of the batched and served objects")
+    ap.add_argument("--hbm-iters", type=int, default=2000, help="iterations timed for roofline_hbm")
     ap.add_argument("--e2e-solves", type=int, default=1,
                     help="complete converged solves timed end to end through the C ABI (0: skip)")
     args = ap.parse_args()

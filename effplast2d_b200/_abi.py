@@ -23,6 +23,7 @@ ERR_NODEV = 7
 
 FP64 = 0
 MIXED = 1
+F32_BULK = 2
 
 KERNEL_AUTO = 0
 KERNEL_TILE = 1
@@ -138,13 +139,15 @@ class BatchStats(ctypes.Structure):
         ("rows", c_int32), ("blocks", c_int32),
         ("kernel", c_int32), ("n_tuned", c_int32),
         ("tune_us", c_double * 6),
+        ("n_tunes", c_int32), ("solo_intervals", c_int32),
     ]
 
     def as_dict(self):
         return {"kernel_ms": self.kernel_ms, "wall_ms": self.wall_ms, "launches": self.launches,
                 "all_launches": self.all_launches, "cell_updates": self.cell_updates,
                 "rows": self.rows, "blocks": self.blocks, "kernel": self.kernel,
-                "n_tuned": self.n_tuned, "tune_us": list(self.tune_us)}
+                "n_tuned": self.n_tuned, "tune_us": list(self.tune_us), "n_tunes": self.n_tunes,
+                "solo_intervals": self.solo_intervals}
 
 
 def make_spec(nx, ny, pa, nl, n_time_steps, init_load_value, load_type):

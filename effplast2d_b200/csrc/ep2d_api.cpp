@@ -199,6 +199,33 @@ int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* launches, int64_t
   return EP2D_OK;
 }
 
+int ep2d_track_plastic_zone(ep2d_handle* h, int32_t on) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  EP2D_GUARD({ return h->rve.track_plastic_zone(on != 0); })
+}
+
+int ep2d_iterate_f32(ep2d_handle* h, int64_t n_iter) {
+  if (!h) return fail(EP2D_ERR_ARG, "null handle");
+  if (n_iter < 0) return fail(EP2D_ERR_ARG, "n_iter must be >= 0");
+  if (h->rve.prm.precision != EP2D_F32_BULK)
+    return fail(EP2D_ERR_STATE, "ep2d_iterate_f32 needs a handle created with EP2D_F32_BULK");
+  EP2D_GUARD({
+    int rc = h->rve.enter_f32();
+    if (rc) return rc;
+    rc = h->rve.iterate(n_iter, false);
+    const int rc2 = h->rve.leave_f32();
+    if (rc) return rc;
+    h->rve.f32_iterations += n_iter;
+    return rc2;
+  })
+}
+
+int ep2d_get_f32_iterations(ep2d_handle* h, int64_t* f32_iterations) {
+  if (!h || !f32_iterations) return fail(EP2D_ERR_ARG, "null argument");
+  *f32_iterations = h->rve.f32_iterations;
+  return EP2D_OK;
+}
+
 int ep2d_polar_fields(ep2d_handle* h, double load_value, double* snu_rr, double* snu_ff, double* san_rr,
                       double* san_ff, uint8_t* plastic) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");

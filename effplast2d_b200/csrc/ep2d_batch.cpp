@@ -43,6 +43,9 @@ int validate_config(const ep2d_batch_config& c) {
   if (c.check_every < 2) return fail(EP2D_ERR_ARG, "check_every must be >= 2 in a batch");
   if (c.niter < c.check_every || c.niter % c.check_every != 0)
     return fail(EP2D_ERR_ARG, "niter must be a positive multiple of check_every in a batch");
+  if (c.precision == EP2D_F32_BULK)
+    return fail(EP2D_ERR_ARG, "the FP32 bulk (EP2D_F32_BULK) runs on single-RVE handles only; batches take EP2D_FP64 "
+                              "or EP2D_MIXED");
   if (c.precision != EP2D_FP64 && c.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
   if (c.kernel < EP2D_KERNEL_AUTO || c.kernel > EP2D_KERNEL_STREAM) return fail(EP2D_ERR_ARG, "unknown kernel form");
   if (c.rows != 0) {
@@ -108,6 +111,8 @@ void BatchEngine::fill_stats(ep2d_batch_stats* st) const {
   st->kernel = shape.form == FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;
   st->n_tuned = n_tuned;
   for (int q = 0; q < 6; q++) st->tune_us[q] = tune_us[q];
+  st->n_tunes = n_tunes;
+  st->solo_intervals = solo_intervals;
 }
 
 int BatchEngine::grow(int need) {
@@ -194,6 +199,7 @@ int BatchEngine::add(const ep2d_rve_spec& spec, uint64_t ticket, double submit_s
   }
   bytes_ += footprint(spec);
   tiles_dirty_ = true;
+  set_version_++;
   if (slot_out) *slot_out = slot;
   return EP2D_OK;
 }
@@ -291,10 +297,14 @@ int BatchEngine::autotune(int64_t* k, int64_t n_avail) {
       slot[nc++] = q;
     }
   const int per = 24;  // 4 warm-up + 20 timed launches per candidate
+  tuned_version_ = set_version_;
   if (n_avail < nc * per) {
     tuned = true;
     return EP2D_OK;
   }
+  n_tunes++;
+  n_tuned = 0;
+  for (double& u : tune_us) u = 0.0;
   const bool mixed = cfg.precision == EP2D_MIXED;
   float best = 1e30f;
   IterShape best_shape = shape;
@@ -360,13 +370,74 @@ int BatchEngine::advance(Slot& s, double error) {
   s.rve.reset();  // release the RVE's device memory
   s.used = false;
   tiles_dirty_ = true;
+  set_version_++;
   return EP2D_OK;
+}
+
+// One checkpoint interval of the only active RVE through the single-RVE path: its own
+// kernel shape (shape_of: the segment height that fills the GPU with that one grid, or
+// the tile form), overlapped launches and its own captured graphs.  Every form rounds
+// alike, so the result is the one the batched launches would give.
+int BatchEngine::run_solo_interval(int q) {
+  Slot& s = slots_[q];
+  Rve& r = *s.rve;
+  const int64_t ce = cfg.check_every;
+  r.f.vmax = d_vmax_ + 2 * q;
+  r.shape = shape_of(r.prm, sm_count_);  // always the same shape: its cached graphs stay valid
+  const double ms0 = r.kernel_ms;
+  int rc = r.iterate(ce, true);  // ce - 1 plain launches, then the recording one (cur follows)
+  if (rc) return rc;
+  kernel_ms += r.kernel_ms - ms0;
+  launches += ce;
+  cell_updates += ce * (int64_t)r.g.nx * r.g.ny;
+  solo_intervals++;
+  EP2D_CK(cudaMemcpyAsync(h_vmax_ + 2 * q, d_vmax_ + 2 * q, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          stream));
+  EP2D_CK(cudaStreamSynchronize(stream));
+  finish_interval(false);
+  return EP2D_OK;
+}
+
+// After an interval: every active RVE's checkpoint (convergence test, next time step or
+// load step, retirement).  flip: the interval's launches left the ping-pong parity to
+// be advanced here (batched launches) rather than by the RVE itself.
+void BatchEngine::finish_interval(bool flip) {
+  const int64_t ce = cfg.check_every;
+  for (size_t q = 0; q < slots_.size(); q++) {
+    Slot& s = slots_[q];
+    if (!s.used || s.task.done) continue;
+    if (flip) s.rve->cur ^= (int)(ce & 1);
+    s.task.iters += ce;
+    double vmx, vmy;
+    std::memcpy(&vmx, &h_vmax_[2 * q], sizeof(double));
+    std::memcpy(&vmy, &h_vmax_[2 * q + 1], sizeof(double));
+    const int rc = advance(s, s.rve->error_from_vmax(vmx, vmy));
+    if (rc) {
+      s.task.status = rc;
+      s.task.error = last_error();
+      s.task.done = true;
+      s.task.done_s = now_s();
+      finished_.push_back(s.task);
+      bytes_ -= footprint(s.task.spec);
+      s.rve.reset();
+      s.used = false;
+      tiles_dirty_ = true;
+      set_version_++;
+    }
+  }
 }
 
 int BatchEngine::run_interval() {
   if (active() == 0) return EP2D_OK;
   DeviceScope ds(device);
   const bool mixed = cfg.precision == EP2D_MIXED;
+  const bool pinned = cfg.rows != 0;  // a pinned shape is used for every launch
+  if (!pinned && active() == 1) {
+    for (size_t q = 0; q < slots_.size(); q++)
+      if (slots_[q].used && !slots_[q].task.done) return run_solo_interval((int)q);
+  }
+  // the fastest shape depends on the active set: tune again after it changed
+  if (!pinned && tuned && tuned_version_ != set_version_) tuned = false;
   // entries: geometry, pointers, current ping-pong parity, per-slot vmax
   std::vector<BatchEntry> ents(slots_.size());
   int64_t cells = 0;
@@ -409,27 +480,7 @@ int BatchEngine::run_interval() {
   kernel_ms += ms;
   launches += ce;
   cell_updates += ce * cells;
-  for (size_t q = 0; q < slots_.size(); q++) {
-    Slot& s = slots_[q];
-    if (!s.used || s.task.done) continue;
-    s.rve->cur ^= (int)(ce & 1);
-    s.task.iters += ce;
-    double vmx, vmy;
-    std::memcpy(&vmx, &h_vmax_[2 * q], sizeof(double));
-    std::memcpy(&vmy, &h_vmax_[2 * q + 1], sizeof(double));
-    rc = advance(s, s.rve->error_from_vmax(vmx, vmy));
-    if (rc) {
-      s.task.status = rc;
-      s.task.error = last_error();
-      s.task.done = true;
-      s.task.done_s = now_s();
-      finished_.push_back(s.task);
-      bytes_ -= footprint(s.task.spec);
-      s.rve.reset();
-      s.used = false;
-      tiles_dirty_ = true;
-    }
-  }
+  finish_interval(true);
   return EP2D_OK;
 }
 
@@ -452,6 +503,7 @@ void BatchEngine::abort_all(int status, const std::string& error) {
     s.used = false;
   }
   tiles_dirty_ = true;
+  set_version_++;
 }
 
 // ---- server -------------------------------------------------------------------------

@@ -63,8 +63,10 @@ class BatchEngine {
   IterShape shape{};  // kernel form and rows of the batched launches
   int blocks = 0;
   bool tuned = false;
-  int n_tuned = 0;
-  double tune_us[6] = {0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 32/64/128
+  int n_tuned = 0;   // candidates of the latest tuning run
+  int n_tunes = 0;   // tuning runs
+  int solo_intervals = 0;
+  double tune_us[6] = {0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 16/32/64
   void fill_stats(ep2d_batch_stats* st) const;
 
  private:
@@ -78,6 +80,8 @@ class BatchEngine {
   int rebuild_tiles();  // the work list: tiles or strip segments of every active RVE
   int ensure_graph();
   int launch_plain_run(int64_t k0, int64_t n);
+  int run_solo_interval(int slot);  // one checkpoint interval of the only active RVE
+  void finish_interval(bool flip);  // every active RVE's checkpoint after an interval
   int autotune(int64_t* k, int64_t n_avail);
   int grow(int need);
 
@@ -92,6 +96,8 @@ class BatchEngine {
   unsigned long long* d_vmax_ = nullptr;
   unsigned long long* h_vmax_ = nullptr;
   int cap_slots_ = 0, cap_tiles_ = 0;
+  uint64_t set_version_ = 0;    // bumped whenever an RVE joins or retires
+  uint64_t tuned_version_ = 0;  // set_version_ the current shape was tuned for
   cudaGraphExec_t graph_ = nullptr;
   IterShape graph_shape_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};

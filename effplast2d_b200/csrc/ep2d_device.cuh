@@ -11,6 +11,7 @@
 //   M_MAT    node inside a pore by SetMaterials' test  -> K = 0.01 K0, G = 0.01 G0
 //   M_NODE   node inside a pore by ComputeStress' test -> P = tauXX = tauYY = 0
 //   M_CORNER corner (i, j) inside a pore               -> tauXY = 0
+//   M_MAT_R  M_MAT of node (i + 1, j)                   (the corner's lower-right node)
 // which reproduces K, G (EffPlast2D.cu:708-728) and the kernel masks (:77-97) exactly
 // while moving 1 byte per cell instead of 16 (K, G) plus 8 (P0, identically 0).
 #pragma once
@@ -65,6 +66,7 @@ __global__ void k_mask(Geo g, uint8_t* __restrict__ mask) {
     const double Lx = __dmul_rn(dX, (double)(nX - 1));
     const double Ly = __dmul_rn(dY, (double)(nY - 1));
     if (host_pore_test(x, y, Lx, Ly, N, rad)) m |= M_MAT;
+    if (i + 1 < g.nx && host_pore_test(host_pos(dX, nX - 1, i + 1), y, Lx, Ly, N, rad)) m |= M_MAT_R;
   }
   // ComputeStress' own tests, EffPlast2D.cu:77-97, written as the reference writes them
   // so that the CUDA compiler treats the arithmetic the same way.
@@ -118,6 +120,54 @@ __global__ void k_preload(Geo g, double* ux0, double* ux1, double* uy0, double* 
     const double v = __dadd_rn(zero_first ? 0.0 : uys[q], __dadd_rn(a, b));
     uy0[q] = v;
     uy1[q] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 state <-> FP32 bulk state.  Ua, the affine field of the preloads, at the faces'
+// positions k_preload uses: Ux = Exx x + Exy y, Uy = Eyy y + Exy x (k_preload adds
+// dUxdy to both, EffPlast2D.cu:370-381).  To FP32: u' = U - Ua rounded to float, into
+// both buffers; back: U = Ua + u', into both buffers.  The velocities are float in both
+// states and stay where they are.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ double affine_ux(const Geo& g, int i, int j, double Exx, double Exy) {
+  return __dadd_rn(__dmul_rn(host_pos(g.dX, g.nx, i), Exx), __dmul_rn(host_pos(g.dY, g.ny - 1, j), Exy));
+}
+__device__ __forceinline__ double affine_uy(const Geo& g, int i, int j, double Eyy, double Exy) {
+  return __dadd_rn(__dmul_rn(host_pos(g.dY, g.ny, j), Eyy), __dmul_rn(host_pos(g.dX, g.nx - 1, i), Exy));
+}
+
+__global__ void k_to_f32(Geo g, const double* __restrict__ ux, const double* __restrict__ uy, float* ux32a,
+                         float* ux32b, float* uy32a, float* uy32b, double Exx, double Eyy, double Exy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const size_t q = (size_t)j * g.pitch + i;
+  if (i <= g.nx && j < g.ny) {
+    const float v = (float)__dsub_rn(ux[q], affine_ux(g, i, j, Exx, Exy));
+    ux32a[q] = v;
+    ux32b[q] = v;
+  }
+  if (i < g.nx && j <= g.ny) {
+    const float v = (float)__dsub_rn(uy[q], affine_uy(g, i, j, Eyy, Exy));
+    uy32a[q] = v;
+    uy32b[q] = v;
+  }
+}
+
+__global__ void k_from_f32(Geo g, const float* __restrict__ ux32, const float* __restrict__ uy32, double* uxa,
+                           double* uxb, double* uya, double* uyb, double Exx, double Eyy, double Exy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const size_t q = (size_t)j * g.pitch + i;
+  if (i <= g.nx && j < g.ny) {
+    const double v = __dadd_rn(affine_ux(g, i, j, Exx, Exy), (double)ux32[q]);
+    uxa[q] = v;
+    uxb[q] = v;
+  }
+  if (i < g.nx && j <= g.ny) {
+    const double v = __dadd_rn(affine_uy(g, i, j, Eyy, Exy), (double)uy32[q]);
+    uya[q] = v;
+    uyb[q] = v;
   }
 }
 
@@ -316,22 +366,28 @@ __global__ void k_static_fields(Geo g, const double* __restrict__ Ux, const doub
 // tauXYav rotated to polar axes, and the analytic ones
 // -P0 + sign(load) 2 coh (log(sqrt(r)) [+ 1]) / sqrt(2), P0 = 0; zero elsewhere and
 // inside the pore (r < rad).  Output unpadded, node (i, j) at j*nx + i.
+// mask != nullptr: the zone accumulated by the tracking launches (M_YN of the node,
+// M_YC of the corners around it: get_sigma_2D.m:126-138, :170-173); else from the
+// recorded state (J2 at coh after the return, J2XY above coh).
 __global__ void k_polar_fields(Geo g, const double* __restrict__ P, const double* __restrict__ txx,
                                const double* __restrict__ tyy, const double* __restrict__ txyav,
-                               const double* __restrict__ j2, const double* __restrict__ j2xy, double sgn,
-                               double* __restrict__ snrr, double* __restrict__ snff, double* __restrict__ sarr,
-                               double* __restrict__ saff, uint8_t* __restrict__ plast) {
+                               const double* __restrict__ j2, const double* __restrict__ j2xy,
+                               const uint8_t* __restrict__ mask, double sgn, double* __restrict__ snrr,
+                               double* __restrict__ snff, double* __restrict__ sarr, double* __restrict__ saff,
+                               uint8_t* __restrict__ plast) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int nx = g.nx, ny = g.ny;
   if (i >= nx || j >= ny) return;
   const size_t pitch = (size_t)g.pitch, q = j * pitch + i;
   const double coh = g.coh;
-  int count = (j2[q] >= coh * (1.0 - 1e-12)) ? 1 : 0;
+  int count = mask ? ((mask[q] & M_YN) ? 1 : 0) : ((j2[q] >= coh * (1.0 - 1e-12)) ? 1 : 0);
   for (int dj = -1; dj <= 0; dj++)
     for (int di = -1; di <= 0; di++) {
       const int ci = i + di, cj = j + dj;
-      if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1 && j2xy[cj * pitch + ci] > coh) count++;
+      if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1 &&
+          (mask ? (mask[cj * pitch + ci] & M_YC) != 0 : j2xy[cj * pitch + ci] > coh))
+        count++;
     }
   const double x = -0.5 * g.dX * (nx - 1) + g.dX * i;
   const double y = -0.5 * g.dY * (ny - 1) + g.dY * j;
@@ -353,6 +409,14 @@ __global__ void k_polar_fields(Geo g, const double* __restrict__ P, const double
   sarr[o] = ar;
   saff[o] = af;
   plast[o] = (uint8_t)count;
+}
+
+__global__ void k_clear_track(Geo g, uint8_t* __restrict__ mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const size_t q = (size_t)j * g.pitch + i;
+  mask[q] = (uint8_t)(mask[q] & ~(M_YN | M_YC));
 }
 
 // ---------------------------------------------------------------------------------

@@ -39,33 +39,61 @@ constexpr int STREAM_DEPTH = 6;                 // rows of loads in flight per w
 constexpr int STREAM_SLOTS = STREAM_DEPTH + 3;
 
 // One row of a warp's 32 columns, as the ring holds it; m: the aligned 32-bit word of
-// the byte mask that contains the lane's node.
-template <typename TV>
+// the byte mask that contains the lane's node.  TU: displacement type (double; float
+// for the FP32 bulk, whose displacements are perturbations of the affine field), TV:
+// velocity type.
+template <typename TU, typename TV>
 struct StreamRow {
-  double ux[32];
-  double uy[32];
+  TU ux[32];
+  TU uy[32];
   TV vx[32];
   TV vy[32];
   uint32_t m[32];
 };
 
-// Shared memory of one warp: its ring, the 16-entry table of corner_g4 by the material
-// bits of the four nodes around a corner, and (K, 2G) by the material bit of a node.
-template <typename TV>
-struct StreamWarpSmem {
-  StreamRow<TV> ring[STREAM_SLOTS];
-  double g4[16];
-  double2 kg[2];
+// (K, 2G) of a node in the arithmetic type
+template <typename T>
+struct KG2 {
+  T k, g2;
 };
 
-template <typename TV>
-constexpr size_t stream_smem_bytes() {
-  return sizeof(StreamWarpSmem<TV>) * STREAM_WARPS;
+// Shared memory of one warp: its ring and two tables that fold the pore masks into the
+// material constants, so that the interior step needs no select for them:
+//   g4z[c]: corner_g4 of a corner by c = (mask(i,j) & (M_MAT | M_CORNER | M_MAT_R)) |
+//           ((mask(i,j+1) & (M_MAT | M_MAT_R)) << 1), and 0 where the corner is in a pore
+//           (bit 2, M_CORNER) -- the corner trial is then 0 * (...) = 0, as the
+//           reference's tauXY = 0 (EffPlast2D.cu:89-92), up to the sign of the zero;
+//   kgz[m]: (K, 2G) of a node by m = mask & (M_MAT | M_NODE), (0, 0) in a pore (M_NODE):
+//           P and the deviators are then 0 (EffPlast2D.cu:79-85), up to the zero's sign.
+// A zero's sign changes no sum, difference or product the iteration forms from it.
+template <typename TU, typename TV>
+struct StreamWarpSmem {
+  StreamRow<TU, TV> ring[STREAM_SLOTS];
+  TU g4z[32];
+  KG2<TU> kgz[4];
+};
+
+// c = corner table index of the corner (i, j) from the mask bytes of nodes (i, j) and
+// (i, j + 1); the four material bits of g4z's index: bit 0 node (i, j), bit 3 (i+1, j),
+// bit 1 (i, j+1), bit 4 (i+1, j+1); bit 2 the corner's pore bit
+__device__ __forceinline__ int corner_index(int m_j, int m_j1) {
+  return (m_j & (M_MAT | M_CORNER | M_MAT_R)) | ((m_j1 & (M_MAT | M_MAT_R)) << 1);
+}
+__device__ __forceinline__ double g4z_entry(int c, double G0, double Gp) {
+  return (c & 4) ? 0.0 : corner_g4(c & 1, (c >> 3) & 1, (c >> 1) & 1, (c >> 4) & 1, G0, Gp);
 }
 
-__device__ __forceinline__ double shfl_idx(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ __forceinline__ double shfl_dn(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
-__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename TU, typename TV>
+constexpr size_t stream_smem_bytes() {
+  return sizeof(StreamWarpSmem<TU, TV>) * STREAM_WARPS;
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_idx(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <typename T>
+__device__ __forceinline__ T shfl_dn(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ int shfl_dn_i(int v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
 // cp.async of 4, 8 or 16 bytes; with ok == false nothing is read and the destination is
@@ -96,27 +124,48 @@ __device__ __forceinline__ bool stream_interior(int nx, int ny, int strip, int j
   return strip >= 1 && STREAM_COLS * strip + 29 <= nx - 3 && jA >= 3 && jB <= ny - 2;
 }
 
-template <bool PLASTIC, bool RECORD, bool INTERIOR, typename TV>
+// The displacement arrays of a form: FP64 U, or the FP32 bulk's perturbations u'.
+template <typename TU>
+__device__ __forceinline__ TU* u_field(const Fields& f, bool y, int buf);
+template <>
+__device__ __forceinline__ double* u_field<double>(const Fields& f, bool y, int buf) {
+  return y ? f.uy[buf] : f.ux[buf];
+}
+template <>
+__device__ __forceinline__ float* u_field<float>(const Fields& f, bool y, int buf) {
+  return y ? f.uy32[buf] : f.ux32[buf];
+}
+
+// One strip segment.  TU = double: the FP64 stencil (velocities stored as TV); TU =
+// float: the FP32 bulk (arithmetic, u' and V in FP32; a RECORD launch then only folds
+// max|V|, the FP64 convergence check reading it in double).
+template <bool PLASTIC, bool RECORD, bool INTERIOR, typename TU, typename TV, bool TRACK = false>
 __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const int src, const int strip,
-                                            const int jA, const int jB, StreamWarpSmem<TV>& sm, double& vmx,
+                                            const int jA, const int jB, StreamWarpSmem<TU, TV>& sm, double& vmx,
                                             double& vmy) {
+  using T = TU;  // arithmetic type
+  constexpr bool F32 = std::is_same<TU, float>::value;
+  static_assert(!F32 || std::is_same<TV, float>::value, "the FP32 bulk stores velocities in FP32");
+  constexpr bool REC_STRESS = RECORD && !F32;  // the FP32 bulk records no stresses
   const int lane = threadIdx.x & 31;
   const int nx = g.nx, ny = g.ny;
   const int pitch = g.pitch;  // pitch * (ny + 1) < 2^31 (checked on the host)
   const int i = STREAM_COLS * strip - 2 + lane;
   const bool own = INTERIOR ? (lane >= 2 && lane < 2 + STREAM_COLS) : (lane >= 2 && lane < 2 + STREAM_COLS && i < nx);
-  const double* __restrict__ ux = src ? f.ux[1] : f.ux[0];
-  const double* __restrict__ uy = src ? f.uy[1] : f.uy[0];
-  double* __restrict__ uxo = src ? f.ux[0] : f.ux[1];
-  double* __restrict__ uyo = src ? f.uy[0] : f.uy[1];
+  const TU* __restrict__ ux = u_field<TU>(f, false, src);
+  const TU* __restrict__ uy = u_field<TU>(f, true, src);
+  TU* __restrict__ uxo = u_field<TU>(f, false, src ^ 1);
+  TU* __restrict__ uyo = u_field<TU>(f, true, src ^ 1);
   TV* __restrict__ fvx = static_cast<TV*>(f.vx);
   TV* __restrict__ fvy = static_cast<TV*>(f.vy);
   const uint8_t* __restrict__ mask = f.mask;
+  // TRACK: the yield bits go to the same bytes; other lanes only read the low bits,
+  // which the stores leave as they are
+  uint8_t* mask_w = const_cast<uint8_t*>(f.mask);
 
   const bool coln = INTERIOR || (i >= 0 && i < nx);   // column of nodes, Uy, Vy
   const int mshift = 8 * (i & 3);                     // pitch % 32 == 0: byte i & 3 of the word
   const int ln1 = min(lane + 1, 31);                  // the lane of column i + 1 (lane 31: unused)
-  const int mshift1 = 8 * ((i + 1) & 3);
 
   // rows k_first .. k_last pass through the ring: U and the mask are needed up to row
   // r + 1 and V up to row r for steps r = jA - 2 .. jB.  U and V move in column pairs:
@@ -130,23 +179,28 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   const int pc = STREAM_COLS * strip - 2 + 2 * (lane & 15);    // first column of the pair
   const bool pair_in = INTERIOR || (pc >= 0 && pc < pitch);
   const int rows_of = half ? ny + 1 : ny;                      // Uy, Vy: rows 0 .. ny
-  const double* __restrict__ u_src = half ? uy : ux;
+  const TU* __restrict__ u_src = half ? uy : ux;
   const TV* __restrict__ v_src = half ? fvy : fvx;
   auto issue = [&](int k, int slot) {
-    StreamRow<TV>& row = sm.ring[slot];
+    StreamRow<TU, TV>& row = sm.ring[slot];
     const bool ok = pair_in && (INTERIOR || (k >= 0 && k < rows_of));
     const int q = ok ? k * pitch + pc : 0;
-    cp_async_pair_zfill<double>((half ? row.uy : row.ux) + 2 * (lane & 15), u_src + q, ok);
+    cp_async_pair_zfill<TU>((half ? row.uy : row.ux) + 2 * (lane & 15), u_src + q, ok);
     cp_async_pair_zfill<TV>((half ? row.vy : row.vx) + 2 * (lane & 15), v_src + q, ok);
     const bool rm = INTERIOR || (coln && k >= 0 && k < ny);  // nodes
     cp_async_zfill<4>(&row.m[lane], mask + (rm ? ((k * pitch + i) & ~3) : 0), rm);
   };
-  const double rdX = g.rdX, rdY = g.rdY, third = 1.0 / 3.0;
-  const double coh = g.coh, coh2 = g.coh2;
-  const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
+  const T rdX = (T)g.rdX, rdY = (T)g.rdY, third = (T)(1.0 / 3.0);
+  const T coh = (T)g.coh, coh2 = (T)g.coh2;
+  const T dT = (T)g.dT, cX = (T)g.cX, cY = (T)g.cY, dtr = (T)g.dtr;
+  const T exx0 = (T)g.exx0, eyy0 = (T)g.eyy0, exy0 = (T)g.exy0;  // FP32 bulk only
   __syncwarp();  // the previous segment of this warp has stopped reading the tables
-  if (lane < 16) sm.g4[lane] = corner_g4_of_bits(lane, g.G0, g.Gp);
-  if (lane < 2) sm.kg[lane] = make_double2(lane ? g.Kp : g.K0, __dmul_rn(2.0, lane ? g.Gp : g.G0));
+  sm.g4z[lane] = (T)g4z_entry(lane, g.G0, g.Gp);
+  if (lane < 4) {
+    KG2<T> kg{(T)0, (T)0};
+    if (!(lane & M_NODE)) kg = KG2<T>{(T)((lane & M_MAT) ? g.Kp : g.K0), (T)__dmul_rn(2.0, (lane & M_MAT) ? g.Gp : g.G0)};
+    sm.kgz[lane] = kg;
+  }
   __syncwarp();
 
   // Launched as a programmatic dependent of the previous iteration (single-RVE form),
@@ -164,18 +218,17 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
 
   // registers at step r (suffix _r: column i+1, _l: column i-1): U rows r (0) and r+1
   // (p), masks rows r and r+1; U and V of row r-1 and r are read back from the ring
-  double ux0 = 0.0, uxp = 0.0, uy0 = 0.0, uyp = 0.0;
-  double ux0_r = 0.0, uxp_r = 0.0;  // Ux(i+1, r), Ux(i+1, r+1)
-  int mk0 = 0, mkp = 0, mk0_r = 0, mkp_r = 0;
-  int g_lo = 0, g_hi = 0;  // material bits of nodes (i, i+1) in rows r and r+1
+  T ux0 = 0, uxp = 0, uy0 = 0, uyp = 0;
+  T ux0_r = 0, uxp_r = 0;  // Ux(i+1, r), Ux(i+1, r+1)
+  int mkm = 0, mk0 = 0, mkp = 0;  // mask bytes of node i in rows r-1, r and r+1
   // trial stresses: nodes rows r-1 (a) and r (b); corners rows r-3..r (c0..c3)
-  double xa = 0.0, ya = 0.0, pb = 0.0, xb = 0.0, yb = 0.0, pa_ = 0.0;
-  double xb_r = 0.0, yb_r = 0.0;  // node trial row r of column i+1; next step: row r-1
-  double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
-  double c2_l = 0.0;  // corner trial row r-1 of column i-1; next step: row r-2
+  T xa = 0, ya = 0, pb = 0, xb = 0, yb = 0, pa_ = 0;
+  T xb_r = 0, yb_r = 0;  // node trial row r of column i+1; next step: row r-1
+  T c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+  T c2_l = 0;  // corner trial row r-1 of column i-1; next step: row r-2
   // returned stresses: nodes rows r-2 (q) and r-1 (w); corners rows r-2 (cq), r-1 (cw)
-  double pq = 0.0, yq = 0.0, pw = 0.0, xw = 0.0, yw = 0.0, cq = 0.0, cw = 0.0;
-  double cw_l = 0.0;  // returned corner row r-1 of column i-1; next step: row r-2
+  T pq = 0, yq = 0, pw = 0, xw = 0, yw = 0, cq = 0, cw = 0;
+  T cw_l = 0;  // returned corner row r-1 of column i-1; next step: row r-2
 
   // slots of rows k, k-1, k-2
   int s_k = STREAM_SLOTS - 1, s_k1 = STREAM_SLOTS - 2, s_k2 = STREAM_SLOTS - 3;
@@ -187,14 +240,11 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     s_k2 = s_k1;
     s_k1 = s_k;
     s_k = (s_k + 1 == STREAM_SLOTS) ? 0 : s_k + 1;
-    const StreamRow<TV>& row = sm.ring[s_k];
+    const StreamRow<TU, TV>& row = sm.ring[s_k];
     ux0 = uxp; uxp = row.ux[lane];
     ux0_r = uxp_r; uxp_r = row.ux[ln1];
     uy0 = uyp; uyp = row.uy[lane];
-    mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
-    mk0_r = mkp_r; mkp_r = (int)((row.m[ln1] >> mshift1) & 0xffu);
-    g_lo = g_hi;
-    g_hi = (mkp & M_MAT) | ((mkp_r & M_MAT) << 1);
+    mkm = mk0; mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
     if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr);  // the slot of row k-3
     cp_async_commit();
     slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
@@ -213,70 +263,84 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     // every formula (lanes a branch would mask run it in lockstep anyway) and a select
     // keeps the value or its default, so the compiler schedules whole rows as straight
     // code; only the stores are predicated.
-    const double uyp_r = sm.ring[s_k].uy[ln1];
-    double pn, xn, yn, cn;
+    const T uyp_r = sm.ring[s_k].uy[ln1];
+    T pn, xn, yn, cn;
     {
-      const double2 kg = sm.kg[mk0 & M_MAT];
-      double p_, x_, y_;
-      node_trial(__dsub_rn(ux0_r, ux0), __dsub_rn(uyp, uy0), kg.x, kg.y, rdX, rdY, third, p_, x_, y_);
-      const bool node_ok = (INTERIOR || (coln && r >= 0 && r < ny)) && !(mk0 & M_NODE);
-      pn = node_ok ? p_ : 0.0;
-      xn = node_ok ? x_ : 0.0;
-      yn = node_ok ? y_ : 0.0;
-      const double c_ =
-          corner_trial(sm.g4[g_lo | (g_hi << 2)], __dsub_rn(uxp_r, ux0_r), __dsub_rn(uyp_r, uyp), rdX, rdY);
-      const bool corner_ok = (INTERIOR || (i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1)) && !(mk0 & M_CORNER);
-      cn = corner_ok ? c_ : 0.0;
+      const KG2<T> kg = sm.kgz[mk0 & (M_MAT | M_NODE)];  // (0, 0) in a pore
+      const T g4 = sm.g4z[corner_index(mk0, mkp)];      // 0 in a pore
+      T p_, x_, y_, c_;
+      if constexpr (F32) {
+        node_trial(sub_rn(ux0_r, ux0), sub_rn(uyp, uy0), exx0, eyy0, kg.k, kg.g2, rdX, rdY, third, p_, x_, y_);
+        c_ = corner_trial(g4, sub_rn(uxp_r, ux0_r), sub_rn(uyp_r, uyp), exy0, rdX, rdY);
+      } else {
+        node_trial(sub_rn(ux0_r, ux0), sub_rn(uyp, uy0), kg.k, kg.g2, rdX, rdY, third, p_, x_, y_);
+        c_ = corner_trial(g4, sub_rn(uxp_r, ux0_r), sub_rn(uyp_r, uyp), rdX, rdY);
+      }
+      if (INTERIOR) {
+        pn = p_; xn = x_; yn = y_; cn = c_;
+      } else {  // nodes and corners outside the grid: 0
+        const bool node_ok = coln && r >= 0 && r < ny;
+        pn = node_ok ? p_ : (T)0;
+        xn = node_ok ? x_ : (T)0;
+        yn = node_ok ? y_ : (T)0;
+        const bool corner_ok = i >= 0 && i < nx - 1 && r >= 0 && r < ny - 1;
+        cn = corner_ok ? c_ : (T)0;
+      }
     }
-    const double xa_r = xb_r, ya_r = yb_r;
+    const T xa_r = xb_r, ya_r = yb_r;
     pa_ = pb; xa = xb; ya = yb;
     pb = pn; xb = xn; yb = yn;
     xb_r = shfl_dn(xb);
     yb_r = shfl_dn(yb);
-    const double c1_l = c2_l;
+    const T c1_l = c2_l;
     c0 = c1; c1 = c2; c2 = c3; c3 = cn;
     c2_l = shfl_up1(c2);
 
     // ---- return of row j = r - 1
     const int j = r - 1;
-    double tav_o = 0.0, j2_o = 0.0, j2xy_o = 0.0;
-    double cq_l = 0.0;
+    T tav_o = 0, j2_o = 0, j2xy_o = 0;
+    T cq_l = 0;
+    bool yld_n = false, yld_c = false;  // TRACK: node / corner (i, j) yields at this iteration
     if constexpr (STAGE >= 1) {
-      double xr = xa, yr = ya, cr = c2;
+      T xr = xa, yr = ya, cr = c2;
       if (PLASTIC) {
         // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
-        double c00, c10, c01, c11;
+        T c00, c10, c01, c11;
         if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j)
           c00 = c1_l; c10 = c1; c01 = c2_l; c11 = c2;
         } else {
           const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
           const int bsel = min(max(j - 1, 0), ny - 3) - j;
-          const double cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
-          const double cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
+          const T cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
+          const T cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
           const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
           c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
           c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
         }
-        const double tav = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(c00, c10), c01), c11));
-        const double nJ2sq = node_j2sq(xa, ya, tav);
+        const T tav = mul_rn((T)0.25, add_rn(add_rn(add_rn(c00, c10), c01), c11));
+        const T nJ2sq = node_j2sq(xa, ya, tav);
         const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
-        const double fn = node_in ? return_factor(nJ2sq, coh, coh2) : 1.0;
+        const T fn = node_in ? return_factor(nJ2sq, coh, coh2) : (T)1;
         // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
-        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(xa, xa_r), xb), xb_r);
-        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(ya, ya_r), yb), yb_r);
-        const double cJ2sq = corner_j2sq(sx, sy, c2);
+        const T sx = add_rn(add_rn(add_rn(xa, xa_r), xb), xb_r);
+        const T sy = add_rn(add_rn(add_rn(ya, ya_r), yb), yb_r);
+        const T cJ2sq = corner_j2sq(sx, sy, c2);
         const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
-        const double fc = corner_in ? return_factor(cJ2sq, coh, coh2) : 1.0;
-        if (RECORD) {
-          tav_o = node_in ? __dmul_rn(tav, fn) : 0.0;
-          j2_o = !node_in ? 0.0
-                          : (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xa, fn), __dmul_rn(ya, fn), tav_o))
-                                        : __dsqrt_rn(nJ2sq);
-          j2xy_o = corner_in ? __dsqrt_rn(cJ2sq) : 0.0;
+        const T fc = corner_in ? return_factor(cJ2sq, coh, coh2) : (T)1;
+        if (TRACK) {  // J2 > coh from the trial stresses (get_sigma_2D.m:126-138)
+          yld_n = node_in && nJ2sq > coh2;
+          yld_c = corner_in && cJ2sq > coh2;
         }
-        xr = __dmul_rn(xa, fn);
-        yr = __dmul_rn(ya, fn);
-        cr = __dmul_rn(c2, fc);
+        if (REC_STRESS) {
+          tav_o = node_in ? mul_rn(tav, fn) : (T)0;
+          j2_o = !node_in ? (T)0
+                          : (fn != (T)1) ? sqrt_rn(node_j2sq(mul_rn(xa, fn), mul_rn(ya, fn), tav_o))
+                                         : sqrt_rn(nJ2sq);
+          j2xy_o = corner_in ? sqrt_rn(cJ2sq) : (T)0;
+        }
+        xr = mul_rn(xa, fn);
+        yr = mul_rn(ya, fn);
+        cr = mul_rn(c2, fc);
       }
       cq_l = cw_l;
       pq = pw; yq = yw; cq = cw;
@@ -287,18 +351,22 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring.  A face
     // the reference leaves alone gets its old velocity back, unchanged.
     if constexpr (STAGE == 2) {
-      const double pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
-      const StreamRow<TV>& rj = sm.ring[s_k2];
-      const double uxm = rj.ux[lane], uym = rj.uy[lane];
-      const double vxm = (double)rj.vx[lane], vym = (double)rj.vy[lane];
-      const TV vxs = (TV)face_velocity(vxm, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, __dsub_rn(cw_l, cq_l), rdY);
-      const TV vys = (TV)face_velocity(vym, cY, dtr, face_diff(pw, pq, yw, yq), rdY, __dsub_rn(cq, cq_l), rdX);
+      const T pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
+      const StreamRow<TU, TV>& rj = sm.ring[s_k2];
+      const T uxm = rj.ux[lane], uym = rj.uy[lane];
+      const T vxm = (T)rj.vx[lane], vym = (T)rj.vy[lane];
+      const TV vxs = (TV)face_velocity(vxm, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, sub_rn(cw_l, cq_l), rdY);
+      const TV vys = (TV)face_velocity(vym, cY, dtr, face_diff(pw, pq, yw, yq), rdY, sub_rn(cq, cq_l), rdX);
       // the displacement moves by the stored velocity
-      const double vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (double)vxs : vxm;
-      const double vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (double)vys : vym;
-      const double uxn = advance(uxm, vx, dT), uyn = advance(uym, vy, dT);
+      const T vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (T)vxs : vxm;
+      const T vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (T)vys : vym;
+      const T uxn = advance(uxm, vx, dT), uyn = advance(uym, vy, dT);
       if (own) {
         const int q = j * pitch + i;
+        if (TRACK) {  // mkm: the mask byte of node (i, j); only this lane writes it
+          const int bits = (yld_n ? M_YN : 0) | (yld_c ? M_YC : 0);
+          if (bits & ~mkm) mask_w[q] = (uint8_t)(mkm | bits);
+        }
         fvx[q] = (TV)vx;
         fvy[q] = (TV)vy;
         uxo[q] = uxn;
@@ -309,14 +377,16 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
             if (RECORD) vmx = fmax(vmx, fabs((double)rj.vx[lane + 1]));
           }
           if (j == ny - 1) {  // face row ny of Uy/Vy (row k-1 of the ring): never updated
-            const StreamRow<TV>& rj1 = sm.ring[s_k1];
+            const StreamRow<TU, TV>& rj1 = sm.ring[s_k1];
             uyo[ny * pitch + i] = rj1.uy[lane];
             if (RECORD) vmy = fmax(vmy, fabs((double)rj1.vy[lane]));
           }
         }
         if (RECORD) {
-          vmx = fmax(vmx, fabs(vx));
-          vmy = fmax(vmy, fabs(vy));
+          vmx = fmax(vmx, fabs((double)vx));
+          vmy = fmax(vmy, fabs((double)vy));
+        }
+        if (REC_STRESS) {
           f.p[q] = pw;
           f.txx[q] = xw;
           f.tyy[q] = yw;
@@ -342,15 +412,15 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   for (; k <= k_last; k++) step(std::integral_constant<int, 2>{});
 }
 
-template <bool PLASTIC, bool RECORD, typename TV>
+template <bool PLASTIC, bool RECORD, typename TU, typename TV, bool TRACK = false>
 __device__ __forceinline__ void stream_segment(const Geo& g, const Fields& f, int src, int strip, int seg, int seg_h,
-                                               StreamWarpSmem<TV>& sm, double& vmx, double& vmy) {
+                                               StreamWarpSmem<TU, TV>& sm, double& vmx, double& vmy) {
   const int jA = seg * seg_h;
   const int jB = min(jA + seg_h, g.ny);
   if (stream_interior(g.nx, g.ny, strip, jA, jB))
-    stream_task<PLASTIC, RECORD, true, TV>(g, f, src, strip, jA, jB, sm, vmx, vmy);
+    stream_task<PLASTIC, RECORD, true, TU, TV, TRACK>(g, f, src, strip, jA, jB, sm, vmx, vmy);
   else
-    stream_task<PLASTIC, RECORD, false, TV>(g, f, src, strip, jA, jB, sm, vmx, vmy);
+    stream_task<PLASTIC, RECORD, false, TU, TV, TRACK>(g, f, src, strip, jA, jB, sm, vmx, vmy);
 }
 
 template <bool RECORD>
@@ -368,18 +438,18 @@ __device__ __forceinline__ void stream_fold_vmax(double vmx, double vmy, unsigne
 }
 
 // One RVE: warp w of CTA b handles task b * STREAM_WARPS + w = (strip, segment).
-template <bool PLASTIC, bool RECORD, typename TV>
+template <bool PLASTIC, bool RECORD, typename TU, typename TV, bool TRACK = false>
 __global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream(Geo g, Fields f, int src, int nstrips, int nsegs,
                                                                    int seg_h) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StreamWarpSmem<TV>& sm = reinterpret_cast<StreamWarpSmem<TV>*>(smem_raw)[threadIdx.x >> 5];
+  StreamWarpSmem<TU, TV>& sm = reinterpret_cast<StreamWarpSmem<TU, TV>*>(smem_raw)[threadIdx.x >> 5];
   // let the next iteration's grid be scheduled now: it waits for this grid's completion
   // before reading anything (griddepcontrol.wait in stream_task)
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const int task = blockIdx.x * STREAM_WARPS + (threadIdx.x >> 5);
   if (task >= nstrips * nsegs) return;  // whole warp
   double vmx = 0.0, vmy = 0.0;
-  stream_segment<PLASTIC, RECORD, TV>(g, f, src, task % nstrips, task / nstrips, seg_h, sm, vmx, vmy);
+  stream_segment<PLASTIC, RECORD, TU, TV, TRACK>(g, f, src, task % nstrips, task / nstrips, seg_h, sm, vmx, vmy);
   stream_fold_vmax<RECORD>(vmx, vmy, f.vmax);
 }
 
@@ -392,7 +462,7 @@ __global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream_batch(const B
                                                                          const int* __restrict__ nunits, int parity,
                                                                          int seg_h) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StreamWarpSmem<TV>& sm = reinterpret_cast<StreamWarpSmem<TV>*>(smem_raw)[threadIdx.x >> 5];
+  StreamWarpSmem<double, TV>& sm = reinterpret_cast<StreamWarpSmem<double, TV>*>(smem_raw)[threadIdx.x >> 5];
   const int n = *nunits;
   const int nw = gridDim.x * STREAM_WARPS;
   for (int t = blockIdx.x * STREAM_WARPS + (threadIdx.x >> 5); t < n; t += nw) {
@@ -400,8 +470,10 @@ __global__ void __launch_bounds__(32 * STREAM_WARPS) k_iter_stream_batch(const B
     const BatchEntry& e = ents[u.x];
     const int src = e.src0 ^ parity;
     double vmx = 0.0, vmy = 0.0;
-    if (e.plastic) stream_segment<true, RECORD, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
-    else stream_segment<false, RECORD, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
+    if (e.plastic)
+      stream_segment<true, RECORD, double, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
+    else
+      stream_segment<false, RECORD, double, TV>(e.g, e.f, src, u.y & 0xffff, u.y >> 16, seg_h, sm, vmx, vmy);
     stream_fold_vmax<RECORD>(vmx, vmy, e.f.vmax);
   }
 }

@@ -1,5 +1,7 @@
 // ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh,
 // ep2d_iter_f64.cuh (tile form) and ep2d_iter_stream.cuh (stream form).
+#include <type_traits>
+
 #include "ep2d_device.cuh"
 #include "ep2d_iter_f64.cuh"
 #include "ep2d_iter_stream.cuh"
@@ -103,27 +105,34 @@ cudaError_t launch_overlapped(void (*kernel)(KArgs...), int blocks, int threads,
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-template <typename TV>
+template <typename TU, typename TV>
 cudaError_t launch_stream_tv(const Geo& g, const Fields& f, int src, bool plastic, bool record, int seg_h,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, bool track = false) {
   const int nstrips = (g.nx + STREAM_COLS - 1) / STREAM_COLS;
   const int nsegs = (g.ny + seg_h - 1) / seg_h;
   const int blocks = (nstrips * nsegs + STREAM_WARPS - 1) / STREAM_WARPS;
   const int threads = 32 * STREAM_WARPS;
-  const size_t sm = stream_smem_bytes<TV>();
-  if (plastic) {
-    if (record) return launch_overlapped(k_iter_stream<true, true, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
-    return launch_overlapped(k_iter_stream<true, false, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+  const size_t sm = stream_smem_bytes<TU, TV>();
+  if constexpr (std::is_same<TU, double>::value) {
+    if (track && plastic) {
+      if (record)
+        return launch_overlapped(k_iter_stream<true, true, TU, TV, true>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+      return launch_overlapped(k_iter_stream<true, false, TU, TV, true>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+    }
   }
-  if (record) return launch_overlapped(k_iter_stream<false, true, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
-  return launch_overlapped(k_iter_stream<false, false, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+  if (plastic) {
+    if (record) return launch_overlapped(k_iter_stream<true, true, TU, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+    return launch_overlapped(k_iter_stream<true, false, TU, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+  }
+  if (record) return launch_overlapped(k_iter_stream<false, true, TU, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
+  return launch_overlapped(k_iter_stream<false, false, TU, TV>, blocks, threads, sm, stream, g, f, src, nstrips, nsegs, seg_h);
 }
 
 template <typename TV>
 cudaError_t launch_stream_batch_tv(const BatchEntry* ents, const int2* units, const int* nunits, int parity,
                                    bool record, int seg_h, int blocks, cudaStream_t stream) {
   const int threads = 32 * STREAM_WARPS;
-  const size_t sm = stream_smem_bytes<TV>();
+  const size_t sm = stream_smem_bytes<double, TV>();
   // plain launches: the persistent batched grid measured 1.5-3 % slower overlapped
   if (record) k_iter_stream_batch<true, TV><<<blocks, threads, sm, stream>>>(ents, units, nunits, parity, seg_h);
   else k_iter_stream_batch<false, TV><<<blocks, threads, sm, stream>>>(ents, units, nunits, parity, seg_h);
@@ -135,9 +144,9 @@ int stream_occupancy(bool record) {
   int n = 0;
   const cudaError_t e =
       record ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_stream_batch<true, TV>, 32 * STREAM_WARPS,
-                                                             stream_smem_bytes<TV>())
+                                                             stream_smem_bytes<double, TV>())
              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iter_stream_batch<false, TV>, 32 * STREAM_WARPS,
-                                                             stream_smem_bytes<TV>());
+                                                             stream_smem_bytes<double, TV>());
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 }  // namespace
@@ -151,12 +160,13 @@ void shape_units(const IterShape& s, int nx, int ny, int* ux, int* uy) {
 }
 
 cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed,
-                        const IterShape& shape, cudaStream_t stream) {
+                        const IterShape& shape, cudaStream_t stream, bool track) {
   if (shape.form == FORM_STREAM) {
     if (shape.rows < SEG_MIN || shape.rows > SEG_MAX) return cudaErrorInvalidValue;
-    return mixed ? launch_stream_tv<float>(g, f, src, plastic, record, shape.rows, stream)
-                 : launch_stream_tv<double>(g, f, src, plastic, record, shape.rows, stream);
+    return mixed ? launch_stream_tv<double, float>(g, f, src, plastic, record, shape.rows, stream, track)
+                 : launch_stream_tv<double, double>(g, f, src, plastic, record, shape.rows, stream, track);
   }
+  if (track) return cudaErrorInvalidValue;  // the plastic-zone tracking runs the stream form
   const int tile_y = shape.rows;
   if (mixed) {
     if (tile_y == 8) return launch_iter_ty<8, float>(g, f, src, plastic, record, stream);
@@ -166,6 +176,12 @@ cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bo
   if (tile_y == 8) return launch_iter_ty<8, double>(g, f, src, plastic, record, stream);
   if (tile_y == 32) return launch_iter_ty<32, double>(g, f, src, plastic, record, stream);
   return launch_iter_ty<16, double>(g, f, src, plastic, record, stream);
+}
+
+cudaError_t launch_iter_f32(const Geo& g, const Fields& f, int src, bool plastic, bool record, int seg_h,
+                            cudaStream_t stream) {
+  if (seg_h < SEG_MIN || seg_h > SEG_MAX) return cudaErrorInvalidValue;
+  return launch_stream_tv<float, float>(g, f, src, plastic, record, seg_h, stream);
 }
 
 cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* units, const int* nunits, int parity, bool record,
@@ -215,6 +231,22 @@ cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx,
   return cudaGetLastError();
 }
 
+cudaError_t launch_to_f32(const Geo& g, const Fields& f, int src, cudaStream_t stream) {
+  const dim3 block(32, 8);
+  const dim3 grid((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8);
+  k_to_f32<<<grid, block, 0, stream>>>(g, f.ux[src], f.uy[src], f.ux32[0], f.ux32[1], f.uy32[0], f.uy32[1], g.exx0,
+                                       g.eyy0, 0.5 * g.exy0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_from_f32(const Geo& g, const Fields& f, int src, cudaStream_t stream) {
+  const dim3 block(32, 8);
+  const dim3 grid((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8);
+  k_from_f32<<<grid, block, 0, stream>>>(g, f.ux32[src], f.uy32[src], f.ux[0], f.ux[1], f.uy[0], f.uy[1], g.exx0,
+                                         g.eyy0, 0.5 * g.exy0);
+  return cudaGetLastError();
+}
+
 namespace {
 constexpr int kAvgRowsPerBlock = 4;
 int avg_blocks(const Geo& g) {
@@ -258,11 +290,18 @@ cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double*
 }
 
 cudaError_t launch_polar_fields(const Geo& g, const Fields& f, double sgn, double* snrr, double* snff, double* sarr,
-                                double* saff, uint8_t* plast, cudaStream_t stream) {
+                                double* saff, uint8_t* plast, bool accumulated, cudaStream_t stream) {
   const dim3 block(32, 8);
   const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
-  k_polar_fields<<<grid, block, 0, stream>>>(g, f.p, f.txx, f.tyy, f.txyav, f.j2, f.j2xy, sgn, snrr, snff, sarr, saff,
-                                             plast);
+  k_polar_fields<<<grid, block, 0, stream>>>(g, f.p, f.txx, f.tyy, f.txyav, f.j2, f.j2xy, accumulated ? f.mask : nullptr,
+                                             sgn, snrr, snff, sarr, saff, plast);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clear_track(const Geo& g, uint8_t* mask, cudaStream_t stream) {
+  const dim3 block(32, 8);
+  const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
+  k_clear_track<<<grid, block, 0, stream>>>(g, mask);
   return cudaGetLastError();
 }
 

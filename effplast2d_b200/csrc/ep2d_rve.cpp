@@ -68,7 +68,8 @@ int validate_params(const ep2d_params& p) {
   if (p.nl < 1 || p.nl > EP2D_MAX_STEPS) return fail(EP2D_ERR_ARG, "nl (NL) must be in [1, 64]");
   if (p.check_every < 1) return fail(EP2D_ERR_ARG, "check_every must be >= 1");
   if (p.niter < 0) return fail(EP2D_ERR_ARG, "niter must be >= 0");
-  if (p.precision != EP2D_FP64 && p.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
+  if (p.precision != EP2D_FP64 && p.precision != EP2D_MIXED && p.precision != EP2D_F32_BULK)
+    return fail(EP2D_ERR_ARG, "unknown precision");
   for (int k = 0; k < EP2D_NPARS; k++)
     if (!std::isfinite(p.pa[k])) return fail(EP2D_ERR_ARG, "pa[" + std::to_string(k) + "] is not finite");
   if (!(p.pa[0] > 0.0) || !(p.pa[1] > 0.0) || !(p.pa[2] > 0.0))
@@ -315,6 +316,7 @@ int prepare_device(int dev) {
 size_t Rve::footprint(const ep2d_params& p) {
   const size_t fe = field_elems(p);
   size_t b = kFieldArrays * align256(fe * sizeof(double));
+  if (p.precision == EP2D_F32_BULK) b += 4 * align256(fe * sizeof(float));  // u' (ping-pong)
   b += align256(fe);                                     // mask
   b += align256(partial_elems(p) * sizeof(double));      // averaging partials
   b += align256((2 * NAVG + n_samples(p) + 2) * sizeof(double));  // sums, samples, vmax
@@ -328,6 +330,11 @@ void Rve::release() {
   if (device >= 0 && (dmem || stream || h_pin)) {
     DeviceScope ds(device);
     for (auto& ge : gexec_)
+      if (ge) {
+        cudaGraphExecDestroy(ge);
+        ge = nullptr;
+      }
+    for (auto& ge : gexec32_)
       if (ge) {
         cudaGraphExecDestroy(ge);
         ge = nullptr;
@@ -361,6 +368,12 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   int sms = 0;
   EP2D_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   shape = shape_of(p, sms);
+  {
+    ep2d_params ps = p;  // the FP32 bulk always runs the stream form
+    ps.kernel = EP2D_KERNEL_STREAM;
+    ps.rows = 0;
+    f32_rows = shape_of(ps, sms).rows;
+  }
   d = derive(p);
   rc = hole_samples(d, p.nx, p.ny, &holes);
   if (rc) return rc;
@@ -423,6 +436,14 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   f.txyav = arr[10];
   f.j2 = arr[11];
   f.j2xy = arr[12];
+  f.ux32[0] = f.ux32[1] = f.uy32[0] = f.uy32[1] = nullptr;
+  if (p.precision == EP2D_F32_BULK) {  // contiguous with the fields: reset() zeroes them too
+    float** a32[4] = {&f.ux32[0], &f.ux32[1], &f.uy32[0], &f.uy32[1]};
+    for (int a = 0; a < 4; a++) {
+      *a32[a] = reinterpret_cast<float*>(cp);
+      cp += align256(fe * sizeof(float));
+    }
+  }
   uint8_t* mask = reinterpret_cast<uint8_t*>(cp);
   f.mask = mask;
   cp += align256(fe);
@@ -470,8 +491,65 @@ int Rve::reset() {
 }
 
 int Rve::launch_one(bool record) {
-  EP2D_CK(launch_iter(g, f, cur, prm.nl > 1, record, mixed(), shape, stream));
+  if (f32) EP2D_CK(launch_iter_f32(g, f, cur, prm.nl > 1, record, f32_rows, stream));
+  else EP2D_CK(launch_iter(g, f, cur, prm.nl > 1, record, mixed(), shape, stream, track));
   cur ^= 1;
+  return EP2D_OK;
+}
+
+int Rve::track_plastic_zone(bool on) {
+  DeviceScope ds(device);
+  if (on == track) {
+    if (on) {  // restart the accumulation
+      EP2D_CK(launch_clear_track(g, const_cast<uint8_t*>(f.mask), stream));
+      aux_launches += 1;
+    }
+    return EP2D_OK;
+  }
+  for (auto& ge : gexec_)  // captured with the other kernel
+    if (ge) {
+      cudaGraphExecDestroy(ge);
+      ge = nullptr;
+    }
+  if (on) {
+    // the tracking launches are stream-form launches; the RVE keeps that shape while
+    // tracking (both forms round alike)
+    if (shape.form != FORM_STREAM) {
+      shape.form = FORM_STREAM;
+      shape.rows = f32_rows;
+    }
+    EP2D_CK(launch_clear_track(g, const_cast<uint8_t*>(f.mask), stream));
+    aux_launches += 1;
+    tracked = true;
+  } else {
+    int sms = 0;
+    EP2D_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    shape = shape_of(prm, sms);
+  }
+  track = on;
+  return EP2D_OK;
+}
+
+int Rve::enter_f32() {
+  // the affine field of the preloads so far: its strains are the macro strain
+  g.exx0 = ces[0];
+  g.eyy0 = ces[1];
+  g.exy0 = 2.0 * ces[2];
+  for (auto& ge : gexec32_)  // captured with the previous strains
+    if (ge) {
+      cudaGraphExecDestroy(ge);
+      ge = nullptr;
+    }
+  EP2D_CK(launch_to_f32(g, f, cur, stream));
+  aux_launches += 1;
+  f32 = true;
+  return EP2D_OK;
+}
+
+int Rve::leave_f32() {
+  EP2D_CK(launch_from_f32(g, f, cur, stream));
+  aux_launches += 1;
+  f32 = false;
   return EP2D_OK;
 }
 
@@ -482,7 +560,8 @@ int Rve::capture(int parity) {
   cur = parity;
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < kGraphLen && le == cudaSuccess; k++) {
-    le = launch_iter(g, f, cur, prm.nl > 1, false, mixed(), shape, stream);
+    le = f32 ? launch_iter_f32(g, f, cur, prm.nl > 1, false, f32_rows, stream)
+             : launch_iter(g, f, cur, prm.nl > 1, false, mixed(), shape, stream, track);
     cur ^= 1;
   }
   cur = saved;
@@ -491,7 +570,7 @@ int Rve::capture(int parity) {
     if (graph) cudaGraphDestroy(graph);
     return fail(EP2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
   }
-  cudaError_t ie = cudaGraphInstantiate(&gexec_[parity], graph, 0);
+  cudaError_t ie = cudaGraphInstantiate(f32 ? &gexec32_[parity] : &gexec_[parity], graph, 0);
   cudaGraphDestroy(graph);
   if (ie != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
   return EP2D_OK;
@@ -499,12 +578,13 @@ int Rve::capture(int parity) {
 
 int Rve::run_plain(int64_t n) {
   if (n >= kGraphLen) {
-    if (!gexec_[cur]) {
+    cudaGraphExec_t* ge = f32 ? gexec32_ : gexec_;
+    if (!ge[cur]) {
       int rc = capture(cur);
       if (rc) return rc;
     }
     while (n >= kGraphLen) {
-      EP2D_CK(cudaGraphLaunch(gexec_[cur], stream));  // even length: parity unchanged
+      EP2D_CK(cudaGraphLaunch(ge[cur], stream));  // even length: parity unchanged
       n -= kGraphLen;
       launches += kGraphLen;
     }
@@ -665,6 +745,12 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
     int rc = begin_time_step(step, it, lsv, lt, n_time_steps);
     if (rc) return rc;
     ep2d_step_record& r = rec[step][it];
+    // FP32 bulk: the time step starts in the FP32 form (below)
+    if (prm.precision == EP2D_F32_BULK) {
+      rc = enter_f32();
+      if (rc) return rc;
+    }
+    double f32_prev = std::numeric_limits<double>::infinity();
     // iteration loop, EffPlast2D.cu:386-428
     double error = 0.0;
     int64_t iter = 0, iters = prm.niter;
@@ -672,6 +758,12 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
     EP2D_CK(cudaEventRecord(ev_[0], stream));
     while (iter < prm.niter) {
       const int64_t block_end = std::min<int64_t>(prm.niter, (iter / ce + 1) * ce);
+      // the last interval, and with it the stresses the step records, is always FP64
+      if (f32 && block_end == prm.niter) {
+        rc = leave_f32();
+        if (rc) return rc;
+      }
+      const bool in_f32 = f32;
       rc = run_plain(block_end - iter - 1);
       if (rc) return rc;
       rc = reset_vmax();
@@ -679,18 +771,35 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
       rc = launch_one(true);
       if (rc) return rc;
       launches++;
+      if (in_f32) f32_iterations += block_end - iter;
       iter = block_end;
       if (iter % ce == 0) {
         rc = read_error(&error);
         if (rc) return rc;
         checks[step][it].push_back(error);
         r.n_checks++;
+        if (in_f32) {
+          // An FP32 checkpoint never decides convergence.  The FP32 form continues
+          // while its residual falls by more than f32_drop per interval; once it stalls
+          // (its rounding floor, or the slow late decay of the plastic zone) or passes
+          // EITER, the state returns to FP64 and FP64 checkpoints take over.
+          if (!(error < f32_drop * f32_prev) || error < prm.eiter) {
+            rc = leave_f32();
+            if (rc) return rc;
+          }
+          f32_prev = error;
+          continue;
+        }
         if (error < prm.eiter) {
           converged = 1;
           iters = iter;
           break;
         }
       }
+    }
+    if (f32) {  // niter not a multiple of check_every: still FP32 at the end
+      rc = leave_f32();
+      if (rc) return rc;
     }
     EP2D_CK(cudaEventRecord(ev_[1], stream));
     EP2D_CK(cudaEventSynchronize(ev_[1]));
@@ -872,7 +981,7 @@ int Rve::polar_fields(double load_value, double* snrr, double* snff, double* sar
   double* tmp = nullptr;
   EP2D_CK(cudaMallocAsync(&tmp, 4 * nn * sizeof(double) + nn, stream));
   uint8_t* pl = reinterpret_cast<uint8_t*>(tmp + 4 * nn);
-  cudaError_t e = launch_polar_fields(g, f, sgn, tmp, tmp + nn, tmp + 2 * nn, tmp + 3 * nn, pl, stream);
+  cudaError_t e = launch_polar_fields(g, f, sgn, tmp, tmp + nn, tmp + 2 * nn, tmp + 3 * nn, pl, tracked, stream);
   double* outs[4] = {snrr, snff, sarr, saff};
   for (int k = 0; k < 4 && e == cudaSuccess; k++)
     e = cudaMemcpyAsync(outs[k], tmp + k * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, stream);

@@ -121,7 +121,20 @@ class Rve {
   Geo g{};
   Fields f{};
   IterShape shape{};  // form and rows of the iteration kernel (shape_of(prm))
-  bool mixed() const { return prm.precision == EP2D_MIXED; }
+  // velocities stored in FP32 (the mixed path, and both phases of the FP32 bulk)
+  bool mixed() const { return prm.precision == EP2D_MIXED || prm.precision == EP2D_F32_BULK; }
+  // FP32 bulk: true while the state is in its FP32 form (u' in f.ux32/uy32)
+  bool f32 = false;
+  int f32_rows = SEG_DEFAULT;        // segment height of the FP32 launches (stream form)
+  double f32_drop = 0.7;             // stay in FP32 while error_k < f32_drop * error_(k-1)
+  int64_t f32_iterations = 0;        // iterations run in FP32
+  // plastic zone of get_sigma_2D.m (:126-138): with track on, every FP64 iteration marks
+  // the nodes and corners whose trial J2 exceeds coh (mask bits M_YN, M_YC); turning it
+  // on clears the marks; polar_fields then uses them (tracked)
+  bool track = false, tracked = false;
+  int track_plastic_zone(bool on);
+  int enter_f32();                   // FP64 U -> u' (at the start of a time step)
+  int leave_f32();                   // u' -> FP64 U
   int cur = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -155,6 +168,7 @@ class Rve {
   int run_plain(int64_t n);
   int capture(int parity);
   cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec32_[2] = {nullptr, nullptr};  // FP32 bulk (hold the affine strains)
   static constexpr int kGraphLen = 64;  // iterations per captured graph (even)
   cudaEvent_t ev_[2] = {nullptr, nullptr};
 };

@@ -59,12 +59,6 @@ __device__ __forceinline__ double return_factor(double j2sq, double coh, double 
   return (j2sq > coh2) ? __dmul_rn(coh, rsqrt(j2sq)) : 1.0;
 }
 
-// corner_g4 for the 16 combinations of the four nodes' material bits, bit b of `bits`
-// being node b in the order m00, m10, m01, m11; equal to corner_g4 bit for bit.
-__device__ __forceinline__ double corner_g4_of_bits(int bits, double G0, double Gp) {
-  return corner_g4(bits & 1, (bits >> 1) & 1, (bits >> 2) & 1, (bits >> 3) & 1, G0, Gp);
-}
-
 // ComputeDisp (:3-35): damped momentum update of one face velocity,
 // v (1 - dt damp) + dt/rho (dA rA + dB rB).
 __device__ __forceinline__ double face_velocity(double v, double c, double dtr, double dA, double rA, double dB,
@@ -79,5 +73,54 @@ __device__ __forceinline__ double face_diff(double p, double p_n, double t, doub
 
 // U += V dt
 __device__ __forceinline__ double advance(double u, double v, double dT) { return __fma_rn(v, dT, u); }
+
+// ---- FP32 bulk ------------------------------------------------------------------
+// The same formulas in FP32 (__f*_rn: neither contracted nor reordered), for the FP32
+// stencil bulk.  Its displacements are the perturbation u' = U - Ua of the affine field
+// Ua = (Exx x + Exy y, Eyy y) the preloads have applied (EffPlast2D.cu:349-381), held as
+// three FP64 scalars: the strain of Ua is exactly (Exx, Eyy, Exy), so the node and
+// corner strains are those constants plus the differences of u', which keeps the FP32
+// differences small (u' ~ 1e-2 of U near the pores) instead of cancelling two FP32
+// values of U itself.
+
+__device__ __forceinline__ void node_trial(float dux, float duy, float exx0, float eyy0, float K, float G2, float rdX,
+                                           float rdY, float third, float& p, float& xx, float& yy) {
+  const float exx = __fadd_rn(__fmul_rn(dux, rdX), exx0);
+  const float eyy = __fadd_rn(__fmul_rn(duy, rdY), eyy0);
+  const float divU = __fadd_rn(exx, eyy);
+  p = __fmul_rn(-K, divU);
+  xx = __fmul_rn(G2, __fmaf_rn(-divU, third, exx));
+  yy = __fmul_rn(G2, __fmaf_rn(-divU, third, eyy));
+}
+__device__ __forceinline__ float corner_trial(float g4, float dxy, float dyx, float exy0, float rdX, float rdY) {
+  return __fmul_rn(g4, __fadd_rn(__fmaf_rn(dxy, rdY, __fmul_rn(dyx, rdX)), exy0));
+}
+__device__ __forceinline__ float node_j2sq(float xx, float yy, float tav) {
+  return __fmaf_rn(xx, xx, __fmaf_rn(yy, yy, __fmul_rn(2.0f, __fmul_rn(tav, tav))));
+}
+__device__ __forceinline__ float corner_j2sq(float sx, float sy, float t) {
+  return __fmaf_rn(__fmul_rn(0.0625f, sx), sx,
+                   __fmaf_rn(__fmul_rn(0.0625f, sy), sy, __fmul_rn(2.0f, __fmul_rn(t, t))));
+}
+__device__ __forceinline__ float return_factor(float j2sq, float coh, float coh2) {
+  return (j2sq > coh2) ? __fmul_rn(coh, rsqrtf(j2sq)) : 1.0f;
+}
+__device__ __forceinline__ float face_velocity(float v, float c, float dtr, float dA, float rA, float dB, float rB) {
+  return __fmaf_rn(v, c, __fmul_rn(dtr, __fmaf_rn(dA, rA, __fmul_rn(dB, rB))));
+}
+__device__ __forceinline__ float face_diff(float p, float p_n, float t, float t_n) {
+  return __fsub_rn(__fadd_rn(__fsub_rn(p_n, p), t), t_n);
+}
+__device__ __forceinline__ float advance(float u, float v, float dT) { return __fmaf_rn(v, dT, u); }
+
+// explicit IEEE add, subtract, multiply of either precision
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 
 }  // namespace ep2d

@@ -8,7 +8,12 @@
 
 namespace ep2d {
 
-enum : uint8_t { M_MAT = 1, M_NODE = 2, M_CORNER = 4 };
+// mask byte of node (i, j): M_MAT, M_NODE, M_CORNER as below (ep2d_device.cuh), and
+// M_MAT_R = the M_MAT bit of node (i + 1, j) (0 on the last column), so that a corner's
+// four material bits come from the two mask bytes of its column
+// M_YN, M_YC: set by the plastic-zone tracking launches when the trial J2 of node (i, j)
+// / corner (i, j) has exceeded coh at some iteration (get_sigma_2D.m's Plast, PlastXY)
+enum : uint8_t { M_MAT = 1, M_NODE = 2, M_CORNER = 4, M_MAT_R = 8, M_YN = 16, M_YC = 32 };
 
 // Per-RVE scalars, passed to kernels by value.
 struct Geo {
@@ -19,6 +24,9 @@ struct Geo {
   // host-computed factors of the iteration kernel: 1/dX, 1/dY, coh^2,
   // 1 - dT dampX, 1 - dT dampY, dT / rho
   double rdX, rdY, coh2, cX, cY, dtr;
+  // FP32 bulk only: strains of the affine field Ua its displacements are measured from:
+  // exx0 = dUa_x/dx, eyy0 = dUa_y/dy, exy0 = dUa_x/dy + dUa_y/dx (= 2 Exy)
+  double exx0, eyy0, exy0;
 };
 
 // Device pointers of one RVE.  Velocities are stored as double on the FP64 path and as
@@ -31,6 +39,9 @@ struct Fields {
   double *p, *txx, *tyy, *txy, *txyav, *j2, *j2xy;  // last recorded stress state
   const uint8_t* mask;
   unsigned long long* vmax;  // [2]: bit patterns of max|Vx|, max|Vy| (non-negative)
+  // FP32 bulk only: the displacement perturbations u' = U - Ua (ping-pong), float
+  float* ux32[2];
+  float* uy32[2];
 };
 
 // One RVE of a batched launch.
@@ -54,7 +65,7 @@ enum IterForm { FORM_TILE = 0, FORM_STREAM = 1 };
 constexpr int STREAM_COLS = 28;  // columns a warp of the stream form owns (32 lanes, 2-lane halos)
 constexpr int SEG_MIN = 16, SEG_MAX = 1024;
 constexpr int SEG_DEFAULT = 64;
-constexpr int SEG_CHOICES[3] = {32, 64, 128};
+constexpr int SEG_CHOICES[3] = {16, 32, 64};  // the batch autotuner's stream-form candidates
 struct IterShape {
   int form = FORM_STREAM;
   int rows = SEG_DEFAULT;
@@ -75,9 +86,21 @@ cudaError_t prepare_kernels();  // per-device function attributes
 cudaError_t launch_mask(const Geo& g, uint8_t* mask, cudaStream_t stream);
 cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx, double dUydy, double dUxdy,
                            int zero_first, cudaStream_t stream);
-// one iteration of one RVE; mixed: velocities stored as float
+// one iteration of one RVE; mixed: velocities stored as float; track: also mark the
+// nodes and corners that yield (M_YN, M_YC; stream form and plastic iterations only)
 cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed,
-                        const IterShape& shape, cudaStream_t stream);
+                        const IterShape& shape, cudaStream_t stream, bool track = false);
+// clear the M_YN / M_YC bits of every node
+cudaError_t launch_clear_track(const Geo& g, uint8_t* mask, cudaStream_t stream);
+// one iteration of the FP32 bulk (stream form, segments of seg_h rows): u' and V in
+// f.ux32/uy32 and f.vx/vy (float), affine strains in g.exx0/eyy0/exy0; a recording launch
+// folds max|V| only
+cudaError_t launch_iter_f32(const Geo& g, const Fields& f, int src, bool plastic, bool record, int seg_h,
+                            cudaStream_t stream);
+// the FP64 state U (buffer src) to the FP32 bulk's u' (both buffers), and back (u'
+// buffer src to both U buffers), with the affine strains of g
+cudaError_t launch_to_f32(const Geo& g, const Fields& f, int src, cudaStream_t stream);
+cudaError_t launch_from_f32(const Geo& g, const Fields& f, int src, cudaStream_t stream);
 // one iteration of every RVE in the work list {rve, x | y << 16} (tiles or strip
 // segments of `shape`), by a persistent grid of `blocks` CTAs
 cudaError_t launch_iter_batch(const BatchEntry* ents, const int2* units, const int* nunits, int parity, bool record,
@@ -93,8 +116,9 @@ cudaError_t launch_gather(const Geo& g, const Fields& f, int src, const unsigned
                           double* out, cudaStream_t stream);
 cudaError_t launch_static_fields(const Geo& g, const Fields& f, int src, double* unu, double* j1, double* j2,
                                  cudaStream_t stream);
+// accumulated: the zone from the M_YN / M_YC bits, else from the recorded J2, J2XY
 cudaError_t launch_polar_fields(const Geo& g, const Fields& f, double sgn, double* snrr, double* snff, double* sarr,
-                                double* saff, uint8_t* plast, cudaStream_t stream);
+                                double* saff, uint8_t* plast, bool accumulated, cudaStream_t stream);
 
 // Scalars of the analytic static solution (SaveAnStatic2D, EffPlast2D.cu:1062-1078).
 struct AnParams {

@@ -24,7 +24,8 @@ EXPORTS = (
     "ep2d_compute_eff_moduli", "ep2d_static_fields", "ep2d_analytic_fields", "ep2d_abi_sizes", "ep2d_get_stats",
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
     "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc", "ep2d_get_kernel_shape",
-    "ep2d_compute_eff_damping", "ep2d_polar_fields",
+    "ep2d_compute_eff_damping", "ep2d_polar_fields", "ep2d_get_f32_iterations",
+    "ep2d_iterate_f32", "ep2d_track_plastic_zone",
 )
 
 
@@ -63,6 +64,9 @@ def lib():
         L.ep2d_analytic_fields.argtypes = [vp, d, d] + [P(d)] * 7
         L.ep2d_abi_sizes.argtypes = [P(i64), i32]
         L.ep2d_get_stats.argtypes = [vp, P(d), P(i64), P(i64), P(i64)]
+        L.ep2d_get_f32_iterations.argtypes = [vp, P(i64)]
+        L.ep2d_iterate_f32.argtypes = [vp, i64]
+        L.ep2d_track_plastic_zone.argtypes = [vp, i32]
         L.ep2d_batch_solve.argtypes = [P(_abi.BatchConfig), P(_abi.RveSpec), i32, P(_abi.Result),
                                        P(_abi.BatchStats)]
         L.ep2d_rve_footprint.argtypes = [P(_abi.RveSpec), i32]
@@ -162,6 +166,15 @@ class Solver:
     def iterate(self, n):
         _check(lib().ep2d_iterate(self._h, int(n)))
 
+    def track_plastic_zone(self, on=True):
+        """get_sigma_2D.m's plastic zone: mark every node / corner that yields at any
+        iteration from now on (on=True clears the marks); polar_fields then uses them"""
+        _check(lib().ep2d_track_plastic_zone(self._h, 1 if on else 0))
+
+    def iterate_f32(self, n):
+        """n iterations of the FP32 bulk's FP32 form (precision=F32_BULK handles)"""
+        _check(lib().ep2d_iterate_f32(self._h, int(n)))
+
     def solve_step(self, step, load_step_value, load_type, n_time_steps=1):
         lt = np.asarray(load_type, dtype=np.float64)
         recs = (_abi.StepRecord * n_time_steps)()
@@ -234,8 +247,10 @@ class Solver:
         la, cu, al = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _check(lib().ep2d_get_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(cu),
                                     ctypes.byref(al)))
+        f32 = ctypes.c_int64()
+        _check(lib().ep2d_get_f32_iterations(self._h, ctypes.byref(f32)))
         return {"kernel_ms": ms.value, "launches": la.value, "cell_updates": cu.value,
-                "all_launches": al.value}
+                "all_launches": al.value, "f32_iterations": f32.value}
 
     def kernel_shape(self):
         """(kernel form, rows) of the iteration kernel this solver launches"""

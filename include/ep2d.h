@@ -46,8 +46,15 @@ enum {
 /* arithmetic of the pseudo-transient stencil */
 enum {
   EP2D_FP64 = 0,         /* plain path: every field and every operation in FP64 */
-  EP2D_MIXED = 1         /* velocities stored in FP32 (half their HBM traffic); displacements,
+  EP2D_MIXED = 1,        /* velocities stored in FP32 (half their HBM traffic); displacements,
                             stencil arithmetic, residual, averages and moduli in FP64 */
+  EP2D_F32_BULK = 2      /* FP32 stencil bulk: each time step starts in FP32 -- arithmetic,
+                            velocities and the displacement perturbation u' = U - Ua about the
+                            affine preload field Ua (three FP64 strains) -- and iterates there
+                            while its checkpoint residual keeps falling by at least 1/0.7 per
+                            interval; the state then goes back to FP64 displacements (EP2D_MIXED)
+                            for the final decades.  Only FP64 checkpoints decide convergence;
+                            averages, increments and moduli stay FP64.  Single-RVE handles only. */
 };
 
 /* form of the fused iteration kernel (both compute the same iteration, operation for
@@ -97,7 +104,7 @@ typedef struct ep2d_params {
   int32_t check_every;     /* output_step (10'000, EffPlast2D.cu:1608) */
   int64_t niter;           /* NITER */
   double eiter;            /* EITER */
-  int32_t precision;       /* EP2D_FP64 or EP2D_MIXED */
+  int32_t precision;       /* EP2D_FP64, EP2D_MIXED or EP2D_F32_BULK */
   int32_t device;          /* DEVICE_IDX */
   int32_t kernel;          /* EP2D_KERNEL_*; 0 = library's choice (no reference counterpart) */
   int32_t rows;            /* rows per tile / strip segment; 0 = library's choice */
@@ -182,9 +189,13 @@ typedef struct ep2d_batch_stats {
   int32_t rows;           /* rows per tile / strip segment used */
   int32_t blocks;         /* persistent grid size (CTAs) */
   int32_t kernel;         /* EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM: the form used */
-  int32_t n_tuned;        /* candidates timed by the autotuner */
-  double tune_us[6];      /* measured us per launch: tile form rows 8, 16, 32, stream form
-                             rows 32, 64, 128 (0 if untimed) */
+  int32_t n_tuned;        /* candidates timed by the latest autotuning run */
+  double tune_us[6];      /* measured us per launch in the latest autotuning run: tile form
+                             rows 8, 16, 32, stream form rows 16, 32, 64 (0 if untimed) */
+  int32_t n_tunes;        /* autotuning runs: one when the batch starts, and one whenever
+                             the set of active RVEs has changed at a checkpoint */
+  int32_t solo_intervals; /* checkpoint intervals run with a single active RVE, through
+                             the single-RVE path (its own kernel shape, overlapped launches) */
 } ep2d_batch_stats;
 
 /* ---- library ---------------------------------------------------------------- */
@@ -274,14 +285,26 @@ int ep2d_analytic_fields(ep2d_handle* h, double delta_p, double tau_infty, doubl
                          double* error_uabs, double* j1an, double* j2an, double* error_j1,
                          double* error_j2, double stats[6]);
 
+/* Plastic-zone tracking as the reference's CPU solver does it (get_sigma_2D.m:126-138):
+ * on = 1 clears the zone and, from then on, every iteration marks each node and corner
+ * whose trial J2 exceeds coh (Plast(iPlast) = 1, PlastXY(iPlastXY) = 1); the marks
+ * accumulate over iterations, time steps and load steps until tracking is turned on
+ * again (cleared) or off (kept).  While tracking, the handle launches the stream form of
+ * the iteration kernel (tracking instantiation; results unchanged, both forms round
+ * alike) and the FP32 phase of EP2D_F32_BULK marks nothing.  ep2d_polar_fields uses the
+ * accumulated zone once tracking has been turned on.  No counterpart in the reference's
+ * CUDA path. */
+int ep2d_track_plastic_zone(ep2d_handle* h, int32_t on);
+
 /* The plastic zone and the stresses in polar coordinates about the grid centre (the pore
  * of a single-pore RVE) that the reference's CPU solver computes after its solve
- * (get_sigma_2D.m:170-194), here from the state the last iteration recorded.  Every
- * output is nx*ny, node (i, j) at j*nx + i:
- *   plastic: 1 if the node yields (recorded J2 reached coh) plus the number of yielding
- *            corners (recorded trial J2XY > coh) among the four around it, as
- *            Plast + PlastXY there; the reference's CPU solver counts a node or corner
- *            that yielded at any iteration, this the final state's;
+ * (get_sigma_2D.m:170-194), from the state the last iteration recorded.  Every output is
+ * nx*ny, node (i, j) at j*nx + i:
+ *   plastic: Plast + PlastXY of get_sigma_2D.m:170-173: 1 if the node yielded plus the
+ *            number of yielded corners among the four around it.  With tracking on
+ *            (ep2d_track_plastic_zone) "yielded" means at any tracked iteration, as the
+ *            CPU solver counts it; without, in the final state (recorded J2 at coh,
+ *            recorded trial J2XY > coh);
  *   snu_rr, snu_ff: tauXX - P, tauYY - P, tauXYav rotated to the polar axes, where
  *            plastic > 0;
  *   san_rr, san_ff: -P0 + sign(load_value) 2 coh (log(sqrt(r)) [+ 1]) / sqrt(2), P0 = 0,
@@ -362,6 +385,15 @@ int ep2d_abi_sizes(int64_t* out, int32_t n);
  * preload, reductions and gathers).  Any pointer may be NULL. */
 int ep2d_get_stats(ep2d_handle* h, double* kernel_ms, int64_t* iter_launches, int64_t* cell_updates,
                    int64_t* all_launches);
+/* n_iter pseudo-time iterations of the FP32 form of EP2D_F32_BULK from the current state
+ * (handles created with EP2D_F32_BULK only, else EP2D_ERR_STATE): the FP64 displacements
+ * go to the FP32 perturbation about the affine field of the current macro strain, the
+ * iterations run, and the state comes back to FP64.  No convergence check; the device time
+ * is added to ep2d_get_stats' kernel_ms.  No counterpart in the reference (all FP64). */
+int ep2d_iterate_f32(ep2d_handle* h, int64_t n_iter);
+/* Iterations this handle has run in the FP32 form of EP2D_F32_BULK (0 for the other
+ * precisions).  No counterpart in the reference (all FP64). */
+int ep2d_get_f32_iterations(ep2d_handle* h, int64_t* f32_iterations);
 /* The iteration kernel this handle launches: EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM and
  * its rows per tile / strip segment (the parameters' choice, or the library's).  No
  * counterpart in the reference. */

@@ -49,6 +49,8 @@ def lib():
         L.orc_compute_eff_damping.argtypes = [vp, d, P(d), i32, d, P(ctypes.c_int64)]
         L.orc_static_fields.argtypes = [vp, d, d] + [P(d)] * 9 + [P(d)]
         L.orc_get_masks.argtypes = [vp, P(ctypes.c_uint8), P(ctypes.c_uint8)]
+        L.orc_track_plastic_zone.argtypes = [vp, i32]
+        L.orc_polar_fields.argtypes = [vp, d, P(d), P(d), P(d), P(d), P(ctypes.c_uint8)]
         _lib = L
     return _lib
 
@@ -175,6 +177,21 @@ class Oracle:
         rc = lib().orc_get_masks(self._h, node.ctypes.data_as(u8), corner.ctypes.data_as(u8))
         assert rc == 0
         return node, corner
+
+    def track_plastic_zone(self, on=True):
+        assert lib().orc_track_plastic_zone(self._h, 1 if on else 0) == 0
+
+    def polar_fields(self, load_value):
+        """get_sigma_2D.m:170-194 with the zone tracked since track_plastic_zone(True):
+        dict of Snurr, Snuff, Sanrr, Sanff (ny x nx) and Plast (counts)"""
+        out = {k: np.zeros((self.ny, self.nx)) for k in ("Snurr", "Snuff", "Sanrr", "Sanff")}
+        plast = np.zeros((self.ny, self.nx), dtype=np.uint8)
+        rc = lib().orc_polar_fields(self._h, float(load_value), *[_dptr(out[k]) for k in
+                                                                  ("Snurr", "Snuff", "Sanrr", "Sanff")],
+                                    plast.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        assert rc == 0
+        out["Plast"] = plast
+        return out
 
     def static_fields(self, delta_p, tau_infty):
         nx, ny = self.nx, self.ny

@@ -54,6 +54,10 @@ struct orc_state {
   /* host copies (the *_cpu arrays after their D2H copies) */
   double *hP, *htauXX, *htauYY, *htauXY, *hUx, *hUy;
   uint8_t *node_in, *corner_in;
+  /* get_sigma_2D.m's Plast / PlastXY (:64-65, set at :126-138): 1 where the trial J2 has
+   * exceeded coh at any iteration since tracking began */
+  int track;
+  uint8_t *plast, *plast_xy;
   /* step records (EffPlast2D.h:108-117) */
   int nts[NSTEP_MAX];
   ep2d_step_record rec[NSTEP_MAX][NT_MAX];
@@ -207,6 +211,9 @@ int orc_create(const ep2d_params* p, orc_state** out) {
   s->hUx = zalloc(nux); s->hUy = zalloc(nuy);
   s->node_in = (uint8_t*)calloc(nn, 1);
   s->corner_in = (uint8_t*)calloc(nc, 1);
+  s->plast = (uint8_t*)calloc(nn, 1);
+  s->plast_xy = (uint8_t*)calloc(nc ? nc : 1, 1);
+  s->track = 0;
   set_materials(s);
   for (int j = 0; j < nY; j++)
     for (int i = 0; i < nX; i++) s->node_in[j * nX + i] = (uint8_t)kernel_node_in(s, i, j);
@@ -226,6 +233,8 @@ int orc_destroy(orc_state* s) {
     for (int t = 0; t < NT_MAX; t++) free(s->checks[a][t]);
   free(s->node_in);
   free(s->corner_in);
+  free(s->plast);
+  free(s->plast_xy);
   free(s);
   return EP2D_OK;
 }
@@ -302,13 +311,17 @@ static void k_plast(orc_state* s) {
   for (long j = 0; j < nY; j++) {
     for (long i = 0; i < nX; i++) {
       if (J2[j * nX + i] > coh) {
+        if (s->track) s->plast[j * nX + i] = 1; /* Plast(iPlast) = 1.0, get_sigma_2D.m:130 */
         tauXX[j * nX + i] *= coh / J2[j * nX + i];
         tauYY[j * nX + i] *= coh / J2[j * nX + i];
         tauXYav[j * nX + i] *= coh / J2[j * nX + i];
         J2[j * nX + i] = sqrt(tauXX[j * nX + i] * tauXX[j * nX + i] + tauYY[j * nX + i] * tauYY[j * nX + i] + 2.0 * tauXYav[j * nX + i] * tauXYav[j * nX + i]);
       }
       if (i < nX - 1 && j < nY - 1) {
-        if (J2XY[j * (nX - 1) + i] > coh) tauXY[j * (nX - 1) + i] *= coh / J2XY[j * (nX - 1) + i];
+        if (J2XY[j * (nX - 1) + i] > coh) {
+          if (s->track) s->plast_xy[j * (nX - 1) + i] = 1; /* PlastXY(iPlastXY) = 1.0, :136 */
+          tauXY[j * (nX - 1) + i] *= coh / J2XY[j * (nX - 1) + i];
+        }
       }
     }
   }
@@ -945,6 +958,64 @@ int orc_static_fields(orc_state* s, double deltaP, double tauInfty, double* UnuA
       stats[4] = eJ2max; stats[5] = eJ2avg / eJn;
     } else {
       for (int a = 0; a < 6; a++) stats[a] = NAN;
+    }
+  }
+  return EP2D_OK;
+}
+
+/* ---- plastic zone and polar stresses (get_sigma_2D.m) ------------------------ */
+
+int orc_track_plastic_zone(orc_state* s, int32_t on) {
+  if (!s) return EP2D_ERR_ARG;
+  s->track = on ? 1 : 0;
+  if (on) {
+    memset(s->plast, 0, (size_t)s->nX * s->nY);
+    memset(s->plast_xy, 0, (size_t)(s->nX - 1) * (s->nY - 1));
+  }
+  return EP2D_OK;
+}
+
+/* get_sigma_2D.m:170-194 on the current state, with the zone accumulated since
+ * orc_track_plastic_zone(s, 1): Plast(node) + PlastXY of the (up to) four corners around
+ * it (:170-173), then, where that count is > 0, the numerical stresses rotated to polar
+ * axes about the grid centre (:185-194; sinsin = y/r, coscos = x/r, :74-75) and the
+ * analytic ones (:176-179, P0 = 0 as at :7); every map is 0 inside the centred pore
+ * radius and where the count is 0.  x, y: the node coordinates -L/2 + d i (:18-21),
+ * here -0.5 d (n - 1) + d i.  Outputs nX*nY, row-major with x fastest. */
+int orc_polar_fields(orc_state* s, double load_value, double* snrr, double* snff, double* sarr, double* saff,
+                     uint8_t* count_out) {
+  if (!s || !snrr || !snff || !sarr || !saff || !count_out) return EP2D_ERR_ARG;
+  const long nX = s->nX, nY = s->nY;
+  const double coh = s->pa[8], rad = s->pa[9];
+  const double sgn = (load_value > 0.0) ? 1.0 : (load_value < 0.0 ? -1.0 : 0.0);
+  const double P0 = 0.0; /* get_sigma_2D.m:7 */
+  for (long j = 0; j < nY; j++) {
+    for (long i = 0; i < nX; i++) {
+      const long q = j * nX + i;
+      int count = s->plast[q];
+      for (int dj = -1; dj <= 0; dj++)
+        for (int di = -1; di <= 0; di++) {
+          const long ci = i + di, cj = j + dj;
+          if (ci >= 0 && ci < nX - 1 && cj >= 0 && cj < nY - 1) count += s->plast_xy[cj * (nX - 1) + ci];
+        }
+      const double x = -0.5 * s->dX * (nX - 1) + s->dX * i;
+      const double y = -0.5 * s->dY * (nY - 1) + s->dY * j;
+      const double r = sqrt(x * x + y * y);
+      const double sn = y / r, cs = x / r;
+      double a = 0.0, b = 0.0, ar = 0.0, af = 0.0;
+      if (count > 0) {
+        const double sxx = s->tauXX[q] - s->P[q], syy = s->tauYY[q] - s->P[q], sxy = s->tauXYav[q];
+        a = sxx * cs * cs + 2.0 * sxy * sn * cs + syy * sn * sn;
+        b = sxx * sn * sn - 2.0 * sxy * sn * cs + syy * cs * cs;
+        ar = -P0 + sgn * 2.0 * coh * log(sqrt(r)) / sqrt(2.0);
+        af = -P0 + sgn * 2.0 * coh * (log(sqrt(r)) + 1.0) / sqrt(2.0);
+      }
+      if (r < rad) a = b = ar = af = 0.0;
+      snrr[q] = a;
+      snff[q] = b;
+      sarr[q] = ar;
+      saff[q] = af;
+      count_out[q] = (uint8_t)count;
     }
   }
   return EP2D_OK;

@@ -45,6 +45,13 @@ int orc_static_fields(orc_state* s, double delta_p, double tau_infty,
 /* kernel-level pore masks as evaluated by ComputeStress (EffPlast2D.cu:77-97):
  * node mask nx*ny and corner mask (nx-1)*(ny-1), 1 = inside a pore */
 int orc_get_masks(orc_state* s, uint8_t* node_mask, uint8_t* corner_mask);
+/* get_sigma_2D.m's plastic zone: on = 1 clears Plast/PlastXY and marks, from then on,
+ * every node / corner whose trial J2 exceeds coh at any iteration (:126-138); 0 stops. */
+int orc_track_plastic_zone(orc_state* s, int32_t on);
+/* get_sigma_2D.m:170-194 with that zone: polar stresses (numerical snrr/snff, analytic
+ * sarr/saff) and the Plast count per node. */
+int orc_polar_fields(orc_state* s, double load_value, double* snrr, double* snff, double* sarr, double* saff,
+                     uint8_t* count_out);
 
 #ifdef __cplusplus
 }

@@ -154,3 +154,37 @@ def test_server_fails_every_request_after_an_engine_error(monkeypatch):
         with pytest.raises(ep.EP2DError) as ei:
             srv.submit(specs[0])
         assert ei.value.status == ep.ERR_STATE
+
+
+# Batched-workload-sized RVEs (grid sides 256..1024, pores 1..4, parameters inside the
+# batched workload's ranges: porosity U(0.005, 0.05), Y in [5e-6, 5e-5], preload
+# magnitude in [2e-5, 8e-5]), every time step solved to convergence: the mixed-precision
+# batch against the plain FP64 single-RVE path, RVE by RVE, at the 1e-5 bar.
+LARGE = [
+    # n, pores, porosity, Y, nl, load, load type, time steps
+    (256, 1, 0.01, 5e-5, 3, -2e-5, (0.9, 1.0, 0.3), 1),
+    (512, 2, 0.02, 4e-5, 2, -3e-5, (1.0, 0.8, 0.0), 1),
+    (768, 3, 0.01, 5e-5, 2, -2e-5, (1.0, 1.0, 0.0), 1),
+    (1024, 4, 0.005, 5e-5, 3, -2e-5, (1.0, 0.9, 0.2), 1),
+]
+
+
+def test_batch_mixed_matches_fp64_at_batched_workload_sizes():
+    niter, ce = 2_000_000, 10_000
+    specs = [mk(*s) for s in LARGE]
+    res, st = B.batch_solve(specs, niter=niter, eiter=1e-9, check_every=ce, precision=ep.MIXED)
+    for sp, r in zip(LARGE, res):
+        n, npo, phi, Y, nl, load, lt, nts = sp
+        pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=Y, porosity=phi, n_pores=npo)
+        s = ep.Solver(n, n, pa, nl=nl, niter=niter, eiter=1e-9, check_every=ce)
+        ref = s.compute_eff_moduli(load, list(lt), nts)
+        s.close()
+        assert ref["all_converged"] and r["all_converged"], (sp, ref["total_iterations"], r["total_iterations"])
+        assert r["total_iterations"] == ref["total_iterations"], sp
+        for kind in ("num", "num_per"):
+            for k in ["kphi", "kd"] + (["g"] if nl == 3 else []):
+                a, b = r[kind][k], ref[kind][k]
+                if math.isfinite(b) and b != 0.0:
+                    print("n=%d %s %s: mixed batch %.12g FP64 %.12g rel %.2e" % (n, kind, k, a, b,
+                                                                               abs(a - b) / abs(b)))
+                    assert abs(a - b) <= 1e-5 * abs(b), (sp, kind, k, a, b)

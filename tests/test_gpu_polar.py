@@ -55,3 +55,38 @@ def test_polar_fields_match_restatement(n, nl, lt):
     for k in ("Snurr", "Snuff", "Sanrr", "Sanff"):
         scale = max(np.max(np.abs(ref[k])), 1e-300)
         assert np.max(np.abs(got[k] - ref[k])) <= 1e-12 * scale, k
+
+
+@pytest.mark.parametrize("n,nl,lt,nts", [(96, 2, (1.0, 1.0, 0.0), 2), (64, 3, (1.0, 0.7, 0.3), 1)])
+def test_tracked_plastic_zone_against_oracle(n, nl, lt, nts):
+    # get_sigma_2D.m's semantics: a node / corner is in the zone if its trial J2 exceeded
+    # coh at ANY iteration (Plast(iPlast) = 1 at :130, PlastXY at :136), accumulated over
+    # the time steps; the oracle restates that, and :170-194's polar stresses, in C
+    import oracle
+
+    load = -6e-5
+    pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=1e-5, porosity=0.02, n_pores=1)
+    s = ep.Solver(n, n, pa, nl=nl, niter=20000, eiter=1e-9, check_every=5000)
+    o = oracle.Oracle(n, n, pa, nl=nl, niter=20000, eiter=1e-9, check_every=5000)
+    s.track_plastic_zone(True)
+    o.track_plastic_zone(True)
+    s.solve_step(0, load, list(lt), nts)
+    o.solve_step(0, load, list(lt), nts)
+    got, ref = s.polar_fields(load), o.polar_fields(load)
+    final = polar_numpy(s, pa, load)["Plast"]
+    g_zone, r_zone = got["Plast"] > 0, ref["Plast"] > 0
+    assert r_zone.mean() > 0.01
+    # the accumulated zone contains the final-state zone and is larger (cells that
+    # yielded on the way and unloaded later)
+    assert np.all(g_zone[final > 0])
+    # yield decisions are J2^2 > coh^2 comparisons of values that agree with the oracle to
+    # ~1e-12; a node exactly at the yield surface may fall either way: allow a few
+    mismatch = int(np.sum(got["Plast"] != ref["Plast"]))
+    assert mismatch <= max(2, n * n // 2000), mismatch
+    both = g_zone & r_zone & (got["Plast"] == ref["Plast"])
+    for k in ("Snurr", "Snuff", "Sanrr", "Sanff"):
+        scale = max(np.max(np.abs(ref[k])), 1e-300)
+        assert np.max(np.abs(got[k][both] - ref[k][both])) <= 1e-9 * scale, k
+    # turning tracking on again clears the zone
+    s.track_plastic_zone(True)
+    assert not s.polar_fields(load)["Plast"].any()
