@@ -431,9 +431,10 @@ def run_ours(args, w):
                                              "achieved = 64 B x 2048^2 per launch / CUDA-event time per launch; "
                                              "traffic from the committed ncu capture of this kernel and grid")
             # the metric's batched and served headline, sized to fit this run
-            line["batched"] = batch_object(args.extra_batch, args.seed, args.extra_niter)
-            line["served"] = serve_object(args.extra_requests, args.seed, args.rate, args.extra_niter,
-                                          sides=(256, 512, 768, 1024))
+            sides = tuple(int(x) for x in args.extra_sides.split(","))
+            line["batched"] = batch_object(args.extra_batch, args.seed, args.extra_niter, sides=sides)
+            line["served"] = serve_object(args.extra_requests, args.seed, args.extra_rate, args.extra_niter,
+                                          sides=sides)
     if world > 1:
         import torch.distributed as dist
 
@@ -575,11 +576,39 @@ def batch_object(count, seed, niter, sides=(256, 512, 768, 1024)):
         "max_rel_moduli_error": {k: (max(v) if v else None) for k, v in errs.items()},
         "max_rel_moduli_error_capped": {k: (max(v) if v else None) for k, v in errs_capped.items()},
         "kernel": st["kernel"], "rows": st["rows"], "tunes": st["n_tunes"], "solo_intervals": st["solo_intervals"],
-        "blocks": st["blocks"]}
+        "blocks": st["blocks"],
+        "per_rve": [{"n": r["n"], "nl": r["nl"], "iterations": rs["total_iterations"],
+                     "converged": bool(rb["all_converged"] and rs["all_converged"])}
+                    for r, rb, rs in zip(reqs, res_b, res_s)]}
+
+
+def run_residency(args):
+    """Does keeping an RVE's state on chip pay?  The same batched kernel (stream form,
+    32-row segments, FP64) on batches of 256^2 RVEs whose combined state fits in the
+    126 MB L2 and on batches that do not: cell-update rate and device time per
+    iteration, for fixed iteration counts (no convergence test)."""
+    import effplast2d_b200 as ep
+    from effplast2d_b200 import batch as B
+
+    out = []
+    n = 256
+    pa = make_pa({"n": n, "g0": 0.5, "yield_stress": 1e-5, "porosity": 0.02, "n_pores": 3})
+    for count in (8, 32, 128, 512):
+        specs = [B.spec(n, pa, 2, 1, -6e-5, (1.0, 1.0, 0.0)) for _ in range(count)]
+        iters = 20_000
+        _, st = B.batch_solve(specs, niter=iters, eiter=0.0, check_every=10_000, kernel=ep.KERNEL_STREAM, rows=32)
+        state = count * 13 * 8 * (n + 1) * (n + 1)
+        out.append({"rves": count, "state_mb": state / 1e6, "l2_resident": state < 126e6,
+                    "us_per_iteration": 1000.0 * st["kernel_ms"] / st["launches"],
+                    "cell_updates_per_s": st["cell_updates"] / (st["kernel_ms"] / 1000.0)})
+    print(json.dumps({"workload": "residency", "grid": "%dx%d" % (n, n), "kernel": "stream, 32-row segments, FP64",
+                      "runs": out}))
+    return 0
 
 
 def run_batch(args):
-    print(json.dumps(dict(workload="batch", **batch_object(args.batch_size, args.seed, args.niter))))
+    sides = tuple(int(x) for x in args.sides.split(",")) if args.sides else (256, 512, 768, 1024)
+    print(json.dumps(dict(workload="batch", **batch_object(args.batch_size, args.seed, args.niter, sides=sides))))
     return 0
 
 
@@ -664,13 +693,17 @@ def serve_object(count, seed, rate, niter, sides=(256, 512, 768, 1024, 2048)):
 
 
 def run_serve(args):
-    print(json.dumps(dict(workload="serve", **serve_object(args.batch_size, args.seed, args.rate, args.niter))))
+    sides = tuple(int(x) for x in args.sides.split(",")) if args.sides else (256, 512, 768, 1024, 2048)
+    print(json.dumps(dict(workload="serve", **serve_object(args.batch_size, args.seed, args.rate, args.niter,
+                                                           sides=sides))))
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch-size", type=int, default=32, help="RVEs of the batch / serve workloads")
+    ap.add_argument("--sides", default="", help="grid sides of the batch / serve workloads, comma-separated "
+                                                "(default 256..1024; serve: up to 2048)")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--rate", type=float, default=1.0, help="request rate of the serve workload (1/s)")
     ap.add_argument("--niter", type=int, default=2_000_000, help="NITER of the batch / serve workloads")
@@ -682,7 +715,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve", "precision"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["batch", "serve", "precision", "residency"])
     ap.add_argument("--precisions", default="mixed,f32_bulk",
                     help="paths --workload precision compares with FP64 (mixed, f32_bulk)")
     ap.add_argument("--precision-workload", default="cfg3", choices=sorted(WORKLOADS),
@@ -693,15 +726,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave the batched, served and roofline_hbm objects out of the default line")
-    ap.add_argument("--extra-batch", type=int, default=8, help="RVEs of the default line's batched object")
-    ap.add_argument("--extra-requests", type=int, default=12, help="requests of the default line's served object")
-    ap.add_argument("--extra-niter", type=int, default=2_000_000, help="NITER of the batched and served objects")
+    ap.add_argument("--extra-batch", type=int, default=16, help="RVEs of the default line's batched object")
+    ap.add_argument("--extra-requests", type=int, default=16, help="requests of the default line's served object")
+    ap.add_argument("--extra-rate", type=float, default=2.0, help="request rate of the served object (1/s)")
+    ap.add_argument("--extra-sides", default="256,512",
+                    help="grid sides of the batched and served objects (the batched workload's distribution "
+                         "restricted to these sides so that both fit the default run)")
+    ap.add_argument("--extra-niter", type=int, default=1_000_000, help="NITER of the batched and served objects")
     ap.add_argument("--hbm-iters", type=int, default=2000, help="iterations timed for roofline_hbm")
     ap.add_argument("--e2e-solves", type=int, default=1,
                     help="complete converged solves timed end to end through the C ABI (0: skip)")
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "residency":
+        return run_residency(args)
     if args.workload == "precision":
         return run_precision(args)
     if args.workload == "serve":

@@ -143,8 +143,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
           double fn = 1.0;
           if (i >= 0 && i < nx && j >= 0 && j < ny) {
             const int a = min(max(i - 1, 0), nx - 3) - (i0 - 2), b = min(max(j - 1, 0), ny - 3) - (j0 - 2);
-            const double tav = __dmul_rn(
-                0.25, __dadd_rn(__dadd_rn(__dadd_rn(s.xy[b][a], s.xy[b][a + 1]), s.xy[b + 1][a]), s.xy[b + 1][a + 1]));
+            const double tav = __dmul_rn(0.25, pair_sum4(s.xy[b][a], s.xy[b][a + 1], s.xy[b + 1][a], s.xy[b + 1][a + 1]));
             const double xv = s.xx[lj][li], yv = s.yy[lj][li];
             const double J2sq = node_j2sq(xv, yv, tav);
             fn = return_factor(J2sq, coh, coh2);
@@ -162,10 +161,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
           const int ci = i0 - 1 + li, cj = j0 - 1 + lj;
           double fc = 1.0;
           if (ci >= 0 && ci < nx - 1 && cj >= 0 && cj < ny - 1) {
-            const double sx =
-                __dadd_rn(__dadd_rn(__dadd_rn(s.xx[lj][li], s.xx[lj][li + 1]), s.xx[lj + 1][li]), s.xx[lj + 1][li + 1]);
-            const double sy =
-                __dadd_rn(__dadd_rn(__dadd_rn(s.yy[lj][li], s.yy[lj][li + 1]), s.yy[lj + 1][li]), s.yy[lj + 1][li + 1]);
+            // column pairs: nodes (i, j) + (i, j+1), then (i+1, j) + (i+1, j+1)
+            const double sx = pair_sum4(s.xx[lj][li], s.xx[lj + 1][li], s.xx[lj][li + 1], s.xx[lj + 1][li + 1]);
+            const double sy = pair_sum4(s.yy[lj][li], s.yy[lj + 1][li], s.yy[lj][li + 1], s.yy[lj + 1][li + 1]);
             const double J2sq = corner_j2sq(sx, sy, s.xy[lj + 1][li + 1]);
             fc = return_factor(J2sq, coh, coh2);
             if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = __dsqrt_rn(J2sq);

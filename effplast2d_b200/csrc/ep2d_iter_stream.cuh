@@ -112,6 +112,19 @@ __device__ __forceinline__ void cp_async_pair_zfill(T* dst, const T* src, bool o
   cp_async_zfill<(int)(2 * sizeof(T))>(dst, src, ok);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// A global store under a predicate, as one predicated instruction.  No later load of
+// the kernel reads these addresses (displacements go to the other ping-pong buffer; a
+// velocity row is read into the ring before its update), so nothing has to be ordered
+// after them.
+__device__ __forceinline__ void st_global_pred(double* p, double v, bool pred) {
+  asm volatile("{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q st.global.f64 [%0], %1;\n}\n" ::"l"(p), "d"(v),
+               "r"((int)pred));
+}
+__device__ __forceinline__ void st_global_pred(float* p, float v, bool pred) {
+  asm volatile("{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q st.global.f32 [%0], %1;\n}\n" ::"l"(p), "f"(v),
+               "r"((int)pred));
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -181,13 +194,15 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   const int rows_of = half ? ny + 1 : ny;                      // Uy, Vy: rows 0 .. ny
   const TU* __restrict__ u_src = half ? uy : ux;
   const TV* __restrict__ v_src = half ? fvy : fvx;
-  auto issue = [&](int k, int slot) {
+  // live == false (rows past the segment's last, k_last): the copies only zero-fill, so
+  // the march issues a row every step without a branch
+  auto issue = [&](int k, int slot, bool live) {
     StreamRow<TU, TV>& row = sm.ring[slot];
-    const bool ok = pair_in && (INTERIOR || (k >= 0 && k < rows_of));
+    const bool ok = live && pair_in && (INTERIOR || (k >= 0 && k < rows_of));
     const int q = ok ? k * pitch + pc : 0;
     cp_async_pair_zfill<TU>((half ? row.uy : row.ux) + 2 * (lane & 15), u_src + q, ok);
     cp_async_pair_zfill<TV>((half ? row.vy : row.vx) + 2 * (lane & 15), v_src + q, ok);
-    const bool rm = INTERIOR || (coln && k >= 0 && k < ny);  // nodes
+    const bool rm = live && (INTERIOR || (coln && k >= 0 && k < ny));  // nodes
     cp_async_zfill<4>(&row.m[lane], mask + (rm ? ((k * pitch + i) & ~3) : 0), rm);
   };
   const T rdX = (T)g.rdX, rdY = (T)g.rdY, third = (T)(1.0 / 3.0);
@@ -211,7 +226,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   int slot_wr = 0;
 #pragma unroll 1
   for (int d = 0; d < STREAM_DEPTH; d++) {
-    if (k_first + d <= k_last) issue(k_first + d, slot_wr);
+    issue(k_first + d, slot_wr, k_first + d <= k_last);
     cp_async_commit();  // empty groups keep the count uniform
     slot_wr++;
   }
@@ -221,11 +236,12 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   T ux0 = 0, uxp = 0, uy0 = 0, uyp = 0;
   T ux0_r = 0, uxp_r = 0;  // Ux(i+1, r), Ux(i+1, r+1)
   int mkm = 0, mk0 = 0, mkp = 0;  // mask bytes of node i in rows r-1, r and r+1
-  // trial stresses: nodes rows r-1 (a) and r (b); corners rows r-3..r (c0..c3)
+  // trial stresses: nodes rows r-1 (a) and r (b); corners rows r-3..r (c0..c3; the
+  // interior needs rows r-1 and r only, with hs1 = the pair sum c(i-1) + c(i) of row r-2)
   T xa = 0, ya = 0, pb = 0, xb = 0, yb = 0, pa_ = 0;
-  T xb_r = 0, yb_r = 0;  // node trial row r of column i+1; next step: row r-1
   T c0 = 0, c1 = 0, c2 = 0, c3 = 0;
   T c2_l = 0;  // corner trial row r-1 of column i-1; next step: row r-2
+  T hs1 = 0;
   // returned stresses: nodes rows r-2 (q) and r-1 (w); corners rows r-2 (cq), r-1 (cw)
   T pq = 0, yq = 0, pw = 0, xw = 0, yw = 0, cq = 0, cw = 0;
   T cw_l = 0;  // returned corner row r-1 of column i-1; next step: row r-2
@@ -245,7 +261,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     ux0_r = uxp_r; uxp_r = row.ux[ln1];
     uy0 = uyp; uyp = row.uy[lane];
     mkm = mk0; mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
-    if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr);  // the slot of row k-3
+    issue(k + STREAM_DEPTH, slot_wr, k + STREAM_DEPTH <= k_last);  // the slot of row k-3
     cp_async_commit();
     slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
   };
@@ -287,14 +303,14 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         cn = corner_ok ? c_ : (T)0;
       }
     }
-    const T xa_r = xb_r, ya_r = yb_r;
     pa_ = pb; xa = xb; ya = yb;
     pb = pn; xb = xn; yb = yn;
-    xb_r = shfl_dn(xb);
-    yb_r = shfl_dn(yb);
     const T c1_l = c2_l;
     c0 = c1; c1 = c2; c2 = c3; c3 = cn;
     c2_l = shfl_up1(c2);
+    // interior: pair sum of row r-1's corners (i-1, i); the previous step's is hs1
+    const T hs0 = hs1;
+    if (INTERIOR && PLASTIC) hs1 = add_rn(c2_l, c2);
 
     // ---- return of row j = r - 1
     const int j = r - 1;
@@ -305,25 +321,27 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       T xr = xa, yr = ya, cr = c2;
       if (PLASTIC) {
         // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
-        T c00, c10, c01, c11;
-        if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j)
-          c00 = c1_l; c10 = c1; c01 = c2_l; c11 = c2;
+        T tav;
+        if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j), rows j-1 and j
+          (void)c1_l;
+          tav = mul_rn((T)0.25, add_rn(hs0, hs1));
         } else {
           const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
           const int bsel = min(max(j - 1, 0), ny - 3) - j;
           const T cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
           const T cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
           const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
-          c00 = shfl_idx(cr0, sa); c10 = shfl_idx(cr0, sb);
-          c01 = shfl_idx(cr1, sa); c11 = shfl_idx(cr1, sb);
+          tav = mul_rn((T)0.25, pair_sum4(shfl_idx(cr0, sa), shfl_idx(cr0, sb), shfl_idx(cr1, sa),
+                                          shfl_idx(cr1, sb)));
         }
-        const T tav = mul_rn((T)0.25, add_rn(add_rn(add_rn(c00, c10), c01), c11));
         const T nJ2sq = node_j2sq(xa, ya, tav);
         const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
         const T fn = node_in ? return_factor(nJ2sq, coh, coh2) : (T)1;
-        // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1)
-        const T sx = add_rn(add_rn(add_rn(xa, xa_r), xb), xb_r);
-        const T sy = add_rn(add_rn(add_rn(ya, ya_r), yb), yb_r);
+        // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1), summed as
+        // column pairs, column i+1's from the next lane
+        const T vx_ = add_rn(xa, xb), vy_ = add_rn(ya, yb);
+        const T sx = add_rn(vx_, shfl_dn(vx_));
+        const T sy = add_rn(vy_, shfl_dn(vy_));
         const T cJ2sq = corner_j2sq(sx, sy, c2);
         const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
         const T fc = corner_in ? return_factor(cJ2sq, coh, coh2) : (T)1;
@@ -361,7 +379,14 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       const T vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (T)vxs : vxm;
       const T vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (T)vys : vym;
       const T uxn = advance(uxm, vx, dT), uyn = advance(uym, vy, dT);
-      if (own) {
+      if constexpr (INTERIOR && !RECORD && !TRACK) {
+        // the common step: four predicated stores, no branch around them
+        const int q = j * pitch + i;
+        st_global_pred(fvx + q, (TV)vx, own);
+        st_global_pred(fvy + q, (TV)vy, own);
+        st_global_pred(uxo + q, uxn, own);
+        st_global_pred(uyo + q, uyn, own);
+      } else if (own) {
         const int q = j * pitch + i;
         if (TRACK) {  // mkm: the mask byte of node (i, j); only this lane writes it
           const int bits = (yld_n ? M_YN : 0) | (yld_c ? M_YC : 0);

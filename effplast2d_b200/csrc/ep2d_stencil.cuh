@@ -6,11 +6,12 @@
 // that calls these functions therefore rounds every cell identically, whatever the
 // surrounding code, the tile or segment shape, or the batch the RVE runs in; results
 // of the kernel forms are equal bit for bit.  The operations follow the reference's
-// expressions (EffPlast2D.cu:37-177) with four rewrites that change rounding only:
+// expressions (EffPlast2D.cu:37-177) with five rewrites that change rounding only:
 // divisions by dX, dY, 3 and rho are multiplications by host-computed reciprocals, the
 // yield test compares J2^2 with coh^2, the return factor coh / J2 is coh * rsqrt(J2^2)
-// (CUDA's double rsqrt, within 1 ulp; the factor within 2 ulp of the quotient), and
-// the marked products and sums are fused.
+// (CUDA's double rsqrt, within 1 ulp; the factor within 2 ulp of the quotient), the
+// four-term sums of the tauXY average and of the corner deviators add two pair sums
+// (pair_sum4) instead of left to right, and the marked products and sums are fused.
 #pragma once
 
 #include "ep2d_types.hpp"
@@ -112,6 +113,17 @@ __device__ __forceinline__ float face_diff(float p, float p_n, float t, float t_
   return __fsub_rn(__fadd_rn(__fsub_rn(p_n, p), t), t_n);
 }
 __device__ __forceinline__ float advance(float u, float v, float dT) { return __fmaf_rn(v, dT, u); }
+
+// The sum of a 2x2 block as two pair sums, (a + b) + (c + d): the tauXY average onto a
+// node (pairs = the block's rows) and the deviator sums onto a corner (pairs = its
+// columns).  Every kernel form adds in this order, so a form may carry a pair sum from
+// one row or lane to the next and still round like the others.
+__device__ __forceinline__ double pair_sum4(double a, double b, double c, double d) {
+  return __dadd_rn(__dadd_rn(a, b), __dadd_rn(c, d));
+}
+__device__ __forceinline__ float pair_sum4(float a, float b, float c, float d) {
+  return __fadd_rn(__fadd_rn(a, b), __fadd_rn(c, d));
+}
 
 // explicit IEEE add, subtract, multiply of either precision
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
