@@ -184,6 +184,7 @@ int BatchEngine::add(const ep2d_rve_spec& spec, uint64_t ticket, double submit_s
     return rc;
   }
   s.rve->shape = shape;
+  s.solo = fills_gpu(*s.rve);
   s.used = true;
   s.task = Task{};
   s.task.spec = spec;
@@ -208,7 +209,7 @@ int BatchEngine::rebuild_tiles() {
   std::vector<int2> tiles;
   for (size_t k = 0; k < slots_.size(); k++) {
     const Slot& s = slots_[k];
-    if (!s.used || s.task.done) continue;
+    if (!s.used || s.task.done || (s.solo && cfg.rows == 0)) continue;
     int tx = 0, ty = 0;
     shape_units(shape, s.rve->g.nx, s.rve->g.ny, &tx, &ty);
     for (int by = 0; by < ty; by++)
@@ -374,39 +375,47 @@ int BatchEngine::advance(Slot& s, double error) {
   return EP2D_OK;
 }
 
-// One checkpoint interval of the only active RVE through the single-RVE path: its own
-// kernel shape (shape_of: the segment height that fills the GPU with that one grid, or
-// the tile form), overlapped launches and its own captured graphs.  Every form rounds
+// True if the RVE keeps the GPU busy alone: its own kernel shape (shape_of) is the stream
+// form with 16 warps' worth of strip segments on every SM.  Such an RVE gains nothing
+// from sharing launches with others and runs its iterations through the single-RVE path
+// (its own shape, overlapped launches, its own captured graphs); smaller ones share the
+// batched launches.
+bool BatchEngine::fills_gpu(const Rve& r) const {
+  const IterShape sh = shape_of(r.prm, sm_count_);
+  if (sh.form != FORM_STREAM) return false;
+  int ux = 0, uy = 0;
+  shape_units(sh, r.g.nx, r.g.ny, &ux, &uy);
+  return (int64_t)ux * uy >= 16 * (int64_t)sm_count_;
+}
+
+// One checkpoint interval of slot q through the single-RVE path: ce - 1 plain launches
+// and the recording one, its max|V| into the slot's pair of d_vmax_.  Every form rounds
 // alike, so the result is the one the batched launches would give.
-int BatchEngine::run_solo_interval(int q) {
+int BatchEngine::run_solo_launches(int q) {
   Slot& s = slots_[q];
   Rve& r = *s.rve;
   const int64_t ce = cfg.check_every;
   r.f.vmax = d_vmax_ + 2 * q;
   r.shape = shape_of(r.prm, sm_count_);  // always the same shape: its cached graphs stay valid
   const double ms0 = r.kernel_ms;
-  int rc = r.iterate(ce, true);  // ce - 1 plain launches, then the recording one (cur follows)
+  const int rc = r.iterate(ce, true);  // cur follows the launches
   if (rc) return rc;
   kernel_ms += r.kernel_ms - ms0;
   launches += ce;
   cell_updates += ce * (int64_t)r.g.nx * r.g.ny;
   solo_intervals++;
-  EP2D_CK(cudaMemcpyAsync(h_vmax_ + 2 * q, d_vmax_ + 2 * q, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                          stream));
-  EP2D_CK(cudaStreamSynchronize(stream));
-  finish_interval(false);
   return EP2D_OK;
 }
 
 // After an interval: every active RVE's checkpoint (convergence test, next time step or
-// load step, retirement).  flip: the interval's launches left the ping-pong parity to
-// be advanced here (batched launches) rather than by the RVE itself.
-void BatchEngine::finish_interval(bool flip) {
+// load step, retirement).  Slots marked `batched` ran the interval in batched launches,
+// which leave the ping-pong parity to be advanced here; the others advanced their own.
+void BatchEngine::finish_interval(const std::vector<char>& batched) {
   const int64_t ce = cfg.check_every;
   for (size_t q = 0; q < slots_.size(); q++) {
     Slot& s = slots_[q];
     if (!s.used || s.task.done) continue;
-    if (flip) s.rve->cur ^= (int)(ce & 1);
+    if (batched[q]) s.rve->cur ^= (int)(ce & 1);
     s.task.iters += ce;
     double vmx, vmy;
     std::memcpy(&vmx, &h_vmax_[2 * q], sizeof(double));
@@ -427,60 +436,80 @@ void BatchEngine::finish_interval(bool flip) {
   }
 }
 
+// One checkpoint interval (check_every iterations) of every active RVE: the RVEs that
+// fill the GPU alone (and a lone RVE of any size) through the single-RVE path, one after
+// another; the others together in batched launches.  A pinned shape batches every RVE.
 int BatchEngine::run_interval() {
   if (active() == 0) return EP2D_OK;
   DeviceScope ds(device);
   const bool mixed = cfg.precision == EP2D_MIXED;
-  const bool pinned = cfg.rows != 0;  // a pinned shape is used for every launch
-  if (!pinned && active() == 1) {
-    for (size_t q = 0; q < slots_.size(); q++)
-      if (slots_[q].used && !slots_[q].task.done) return run_solo_interval((int)q);
-  }
-  // the fastest shape depends on the active set: tune again after it changed
-  if (!pinned && tuned && tuned_version_ != set_version_) tuned = false;
-  // entries: geometry, pointers, current ping-pong parity, per-slot vmax
-  std::vector<BatchEntry> ents(slots_.size());
+  const bool pinned = cfg.rows != 0;
+  const int n_active = active();
+  std::vector<char> batched(slots_.size(), 0);
+  std::vector<int> solo;
+  int n_batched = 0;
   int64_t cells = 0;
-  for (size_t k = 0; k < slots_.size(); k++) {
-    Slot& s = slots_[k];
-    if (!s.used) continue;
-    s.rve->f.vmax = d_vmax_ + 2 * k;
-    ents[k].g = s.rve->g;
-    ents[k].f = s.rve->f;
-    ents[k].src0 = s.rve->cur;
-    ents[k].plastic = s.rve->prm.nl > 1 ? 1 : 0;
-    cells += (int64_t)s.rve->g.nx * s.rve->g.ny;
-  }
-  EP2D_CK(cudaMemcpyAsync(d_ents_, ents.data(), ents.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, stream));
-  if (tiles_dirty_) {
-    const int rc = rebuild_tiles();
-    if (rc) return rc;
-  } else {
-    EP2D_CK(cudaStreamSynchronize(stream));
+  for (size_t q = 0; q < slots_.size(); q++) {
+    const Slot& s = slots_[q];
+    if (!s.used || s.task.done) continue;
+    if (!pinned && (s.solo || n_active == 1)) {
+      solo.push_back((int)q);
+    } else {
+      batched[q] = 1;
+      n_batched++;
+      cells += (int64_t)s.rve->g.nx * s.rve->g.ny;
+    }
   }
   const int64_t ce = cfg.check_every;
-  int64_t k = 0;
-  if (!tuned) {
-    const int rc = autotune(&k, ce - 1);
+  EP2D_CK(cudaMemsetAsync(d_vmax_, 0, slots_.size() * 2 * sizeof(unsigned long long), stream));
+  if (n_batched > 0) {
+    // the fastest shape depends on the batched set: tune again after it changed
+    if (!pinned && tuned && tuned_version_ != set_version_) tuned = false;
+    // entries: geometry, pointers, current ping-pong parity, per-slot vmax
+    std::vector<BatchEntry> ents(slots_.size());
+    for (size_t k = 0; k < slots_.size(); k++) {
+      Slot& s = slots_[k];
+      if (!s.used) continue;
+      s.rve->f.vmax = d_vmax_ + 2 * k;
+      ents[k].g = s.rve->g;
+      ents[k].f = s.rve->f;
+      ents[k].src0 = s.rve->cur;
+      ents[k].plastic = s.rve->prm.nl > 1 ? 1 : 0;
+    }
+    EP2D_CK(cudaMemcpyAsync(d_ents_, ents.data(), ents.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, stream));
+    if (tiles_dirty_) {
+      const int rc = rebuild_tiles();
+      if (rc) return rc;
+    } else {
+      EP2D_CK(cudaStreamSynchronize(stream));
+    }
+    int64_t k = 0;
+    if (!tuned) {
+      const int rc = autotune(&k, ce - 1);
+      if (rc) return rc;
+    }
+    int rc = ensure_graph();
+    if (rc) return rc;
+    EP2D_CK(cudaEventRecord(ev_[0], stream));
+    rc = launch_plain_run(k, ce - 1 - k);
+    if (rc) return rc;
+    EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)((ce - 1) & 1), true, mixed, shape, blocks, stream));
+    EP2D_CK(cudaEventRecord(ev_[1], stream));
+    EP2D_CK(cudaEventSynchronize(ev_[1]));
+    float ms = 0.0f;
+    EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    kernel_ms += ms;
+    launches += ce;
+    cell_updates += ce * cells;
+  }
+  for (int q : solo) {
+    const int rc = run_solo_launches(q);
     if (rc) return rc;
   }
-  int rc = ensure_graph();
-  if (rc) return rc;
-  EP2D_CK(cudaEventRecord(ev_[0], stream));
-  rc = launch_plain_run(k, ce - 1 - k);
-  if (rc) return rc;
-  EP2D_CK(cudaMemsetAsync(d_vmax_, 0, slots_.size() * 2 * sizeof(unsigned long long), stream));
-  EP2D_CK(launch_iter_batch(d_ents_, d_tiles_, d_ntiles_, (int)((ce - 1) & 1), true, mixed, shape, blocks, stream));
-  EP2D_CK(cudaEventRecord(ev_[1], stream));
   EP2D_CK(cudaMemcpyAsync(h_vmax_, d_vmax_, slots_.size() * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           stream));
   EP2D_CK(cudaStreamSynchronize(stream));
-  float ms = 0.0f;
-  EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
-  kernel_ms += ms;
-  launches += ce;
-  cell_updates += ce * cells;
-  finish_interval(true);
+  finish_interval(batched);
   return EP2D_OK;
 }
 

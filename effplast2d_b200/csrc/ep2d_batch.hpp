@@ -65,7 +65,7 @@ class BatchEngine {
   bool tuned = false;
   int n_tuned = 0;   // candidates of the latest tuning run
   int n_tunes = 0;   // tuning runs
-  int solo_intervals = 0;
+  int solo_intervals = 0;  // checkpoint intervals an RVE ran through the single-RVE path
   double tune_us[6] = {0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 16/32/64
   void fill_stats(ep2d_batch_stats* st) const;
 
@@ -74,14 +74,16 @@ class BatchEngine {
     std::unique_ptr<Rve> rve;
     Task task;
     bool used = false;
+    bool solo = false;  // fills the GPU alone: runs through the single-RVE path
   };
   int begin_task_step(Slot& s);
   int advance(Slot& s, double error);  // after a checkpoint of this slot's time step
   int rebuild_tiles();  // the work list: tiles or strip segments of every active RVE
   int ensure_graph();
   int launch_plain_run(int64_t k0, int64_t n);
-  int run_solo_interval(int slot);  // one checkpoint interval of the only active RVE
-  void finish_interval(bool flip);  // every active RVE's checkpoint after an interval
+  bool fills_gpu(const Rve& r) const;  // the RVE keeps the GPU busy on its own
+  int run_solo_launches(int slot);     // one checkpoint interval through the single-RVE path
+  void finish_interval(const std::vector<char>& batched);  // every active RVE's checkpoint
   int autotune(int64_t* k, int64_t n_avail);
   int grow(int need);
 

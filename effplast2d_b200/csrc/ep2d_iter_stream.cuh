@@ -113,18 +113,6 @@ __device__ __forceinline__ void cp_async_pair_zfill(T* dst, const T* src, bool o
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
-// A global store under a predicate, as one predicated instruction.  No later load of
-// the kernel reads these addresses (displacements go to the other ping-pong buffer; a
-// velocity row is read into the ring before its update), so nothing has to be ordered
-// after them.
-__device__ __forceinline__ void st_global_pred(double* p, double v, bool pred) {
-  asm volatile("{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q st.global.f64 [%0], %1;\n}\n" ::"l"(p), "d"(v),
-               "r"((int)pred));
-}
-__device__ __forceinline__ void st_global_pred(float* p, float v, bool pred) {
-  asm volatile("{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q st.global.f32 [%0], %1;\n}\n" ::"l"(p), "f"(v),
-               "r"((int)pred));
-}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -194,8 +182,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   const int rows_of = half ? ny + 1 : ny;                      // Uy, Vy: rows 0 .. ny
   const TU* __restrict__ u_src = half ? uy : ux;
   const TV* __restrict__ v_src = half ? fvy : fvx;
-  // live == false (rows past the segment's last, k_last): the copies only zero-fill, so
-  // the march issues a row every step without a branch
+  // live == false (rows past the segment's last, k_last): the copies only zero-fill
   auto issue = [&](int k, int slot, bool live) {
     StreamRow<TU, TV>& row = sm.ring[slot];
     const bool ok = live && pair_in && (INTERIOR || (k >= 0 && k < rows_of));
@@ -261,7 +248,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     ux0_r = uxp_r; uxp_r = row.ux[ln1];
     uy0 = uyp; uyp = row.uy[lane];
     mkm = mk0; mk0 = mkp; mkp = (int)((row.m[lane] >> mshift) & 0xffu);
-    issue(k + STREAM_DEPTH, slot_wr, k + STREAM_DEPTH <= k_last);  // the slot of row k-3
+    if (k + STREAM_DEPTH <= k_last) issue(k + STREAM_DEPTH, slot_wr, true);  // the slot of row k-3
     cp_async_commit();
     slot_wr = (slot_wr + 1 == STREAM_SLOTS) ? 0 : slot_wr + 1;
   };
@@ -379,14 +366,7 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       const T vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (T)vxs : vxm;
       const T vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (T)vys : vym;
       const T uxn = advance(uxm, vx, dT), uyn = advance(uym, vy, dT);
-      if constexpr (INTERIOR && !RECORD && !TRACK) {
-        // the common step: four predicated stores, no branch around them
-        const int q = j * pitch + i;
-        st_global_pred(fvx + q, (TV)vx, own);
-        st_global_pred(fvy + q, (TV)vy, own);
-        st_global_pred(uxo + q, uxn, own);
-        st_global_pred(uyo + q, uyn, own);
-      } else if (own) {
+      if (own) {
         const int q = j * pitch + i;
         if (TRACK) {  // mkm: the mask byte of node (i, j); only this lane writes it
           const int bits = (yld_n ? M_YN : 0) | (yld_c ? M_YC : 0);

@@ -194,8 +194,9 @@ typedef struct ep2d_batch_stats {
                              rows 8, 16, 32, stream form rows 16, 32, 64 (0 if untimed) */
   int32_t n_tunes;        /* autotuning runs: one when the batch starts, and one whenever
                              the set of active RVEs has changed at a checkpoint */
-  int32_t solo_intervals; /* checkpoint intervals run with a single active RVE, through
-                             the single-RVE path (its own kernel shape, overlapped launches) */
+  int32_t solo_intervals; /* RVE checkpoint intervals run through the single-RVE path (its
+                             own kernel shape, overlapped launches, its own graphs): RVEs
+                             that fill the GPU alone, and a lone active RVE of any size */
 } ep2d_batch_stats;
 
 /* ---- library ---------------------------------------------------------------- */
