@@ -188,3 +188,23 @@ def test_batch_mixed_matches_fp64_at_batched_workload_sizes():
                     print("n=%d %s %s: mixed batch %.12g FP64 %.12g rel %.2e" % (n, kind, k, a, b,
                                                                                abs(a - b) / abs(b)))
                     assert abs(a - b) <= 1e-5 * abs(b), (sp, kind, k, a, b)
+
+
+def test_batch_with_gpu_filling_rve_matches_single_bit_for_bit():
+    # a 1024^2 RVE fills the GPU alone, so the batch runs it through the single-RVE path
+    # while the small ones share batched launches; every path rounds alike, so each RVE
+    # must equal its single-RVE run exactly (iteration-capped steps: NITER 20000)
+    niter, ce = 20000, 10000
+    specs_p = [(1024, 3, 0.01, 1e-5, 2, -6e-5, (1.0, 1.0, 0.0), 1),
+               (96, 3, 0.02, 1e-5, 3, -6e-5, (1.0, 0.8, 0.3), 1),
+               (128, 1, 0.01, 2e-5, 2, -5e-5, (0.9, 1.0, 0.2), 1)]
+    specs = [mk(*s) for s in specs_p]
+    res, st = B.batch_solve(specs, niter=niter, eiter=1e-9, check_every=ce)
+    assert st["solo_intervals"] > 0
+    for sp, r in zip(specs_p, res):
+        n, npo, phi, Y, nl, load, lt, nts = sp
+        pa = ep.make_pa(20.0, 20.0, n, n, g0=0.5, yield_stress=Y, porosity=phi, n_pores=npo)
+        s = ep.Solver(n, n, pa, nl=nl, niter=niter, eiter=1e-9, check_every=ce)
+        ref = s.compute_eff_moduli(load, list(lt), nts)
+        s.close()
+        check_result(r, ref, 0.0, nl)
