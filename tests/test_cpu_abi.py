@@ -92,14 +92,15 @@ def test_solver_without_device_fails_loudly():
 
 
 @pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "side65537", "field_2e31", "zero_pores", "kernel3",
-                                 "tile_rows12", "stream_rows8", "stream_rows2048"])
+                                 "tile_rows12", "stream_rows8", "stream_rows2048", "precision3"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
     pa = ep.make_pa(20.0, 20.0, 32, 32)
     nx, nl = 32, 1
     kw = {"kernel3": dict(kernel=3), "tile_rows12": dict(kernel=ep.KERNEL_TILE, rows=12),
           "stream_rows8": dict(kernel=ep.KERNEL_STREAM, rows=8),
-          "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048)}.get(bad, {})
+          "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048),
+          "precision3": dict(precision=3)}.get(bad, {})
     if bad == "nan_dx":
         pa[0] = float("nan")
     elif bad == "nl65":  # beyond EP2D_MAX_STEPS (nl 4..64 is the damping mode)
@@ -133,3 +134,25 @@ def test_batch_and_server_argument_errors():
     with pytest.raises(ep.EP2DError) as e:
         B.batch_solve([s], niter=2000, check_every=1000, rows=12)
     assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)
+
+
+def test_precisions_accepted_by_validation():
+    # FP64, mixed and the FP32 bulk pass argument validation: without a device the
+    # failure is the missing device, not the argument
+    if ep.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    pa = ep.make_pa(20.0, 20.0, 32, 32)
+    for prec in (ep.FP64, ep.MIXED, ep.F32_BULK):
+        with pytest.raises(ep.EP2DError) as e:
+            ep.Solver(32, 32, pa, precision=prec)
+        assert e.value.status == _abi.ERR_NODEV, prec
+
+
+def test_f32_bulk_footprint_adds_the_perturbation_arrays():
+    from effplast2d_b200 import batch as B
+
+    pa = ep.make_pa(20.0, 20.0, 64, 64)
+    s = B.spec(64, pa, 2, 1, -6e-5, (1.0, 1.0, 0.0))
+    # four float arrays of the common pitch (96 for nx = 64) x 65 rows, 256-byte aligned
+    extra = 4 * (((96 * 65 * 4) + 255) // 256 * 256)
+    assert B.footprint(s, ep.F32_BULK) == B.footprint(s) + extra
