@@ -292,7 +292,6 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     }
     pa_ = pb; xa = xb; ya = yb;
     pb = pn; xb = xn; yb = yn;
-    const T c1_l = c2_l;
     c0 = c1; c1 = c2; c2 = c3; c3 = cn;
     c2_l = shfl_up1(c2);
     // interior: pair sum of row r-1's corners (i-1, i); the previous step's is hs1
@@ -310,7 +309,6 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
         T tav;
         if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j), rows j-1 and j
-          (void)c1_l;
           tav = mul_rn((T)0.25, add_rn(hs0, hs1));
         } else {
           const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
