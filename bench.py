@@ -405,7 +405,10 @@ def run_ours(args, w):
                          "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
                          "kernel": "k_iter_stream (fused stress, J2 return, momentum update)",
                          "algorithmic_bytes_per_launch": bytes_alg, "avg_launch_us": avg_launch_s * 1e6,
-                         "peak_source": peak_kind},
+                         "peak_source": peak_kind,
+                         "note": "the %d^2 state (%.0f MB) is L2-resident within a step, so this fraction "
+                                 "measures throughput against a bound the kernel does not meet here; the "
+                                 "HBM-resident case of the same kernel is roofline_hbm" % (n, 13 * 8 * n * n / 1e6)},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cell_updates_per_s": iters_per_s * n * n,

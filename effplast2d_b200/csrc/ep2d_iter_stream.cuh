@@ -33,7 +33,7 @@
 namespace ep2d {
 
 constexpr int STREAM_WARPS = 4;                 // warps per CTA (STREAM_COLS owned columns per warp)
-constexpr int STREAM_DEPTH = 6;                 // rows of loads in flight per warp
+constexpr int STREAM_DEPTH = 4;                 // rows of loads in flight per warp
 // rows k-2 .. k+DEPTH live in the ring at step k: the faces of row k-2 read U and V of
 // rows k-2 and k-1 from it, and the refill goes to the slot of row k-3
 constexpr int STREAM_SLOTS = STREAM_DEPTH + 3;
