@@ -133,7 +133,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
 
   // ---- C: J2 radial return (NL > 1, EffPlast2D.cu:392-397)
   if (PLASTIC) {
-    const double coh = g.coh, coh2 = g.coh2;
+    const double coh = g.coh, coh2 = g.coh2, coh4 = g.coh4, coh2x16 = g.coh2x16;
 #pragma unroll
     for (int lj = ty; lj < FH; lj += 8) {
 #pragma unroll
@@ -143,12 +143,12 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
           double fn = 1.0;
           if (i >= 0 && i < nx && j >= 0 && j < ny) {
             const int a = min(max(i - 1, 0), nx - 3) - (i0 - 2), b = min(max(j - 1, 0), ny - 3) - (j0 - 2);
-            const double tav = __dmul_rn(0.25, pair_sum4(s.xy[b][a], s.xy[b][a + 1], s.xy[b + 1][a], s.xy[b + 1][a + 1]));
+            const double hsum = pair_sum4(s.xy[b][a], s.xy[b][a + 1], s.xy[b + 1][a], s.xy[b + 1][a + 1]);
             const double xv = s.xx[lj][li], yv = s.yy[lj][li];
-            const double J2sq = node_j2sq(xv, yv, tav);
+            const double J2sq = node_j2sq_h(xv, yv, hsum);
             fn = return_factor(J2sq, coh, coh2);
             if (RECORD && li >= 1 && lj >= 1) {
-              const double tavo = __dmul_rn(tav, fn);
+              const double tavo = __dmul_rn(__dmul_rn(0.25, hsum), fn);
               const double J2o =
                   (fn != 1.0) ? __dsqrt_rn(node_j2sq(__dmul_rn(xv, fn), __dmul_rn(yv, fn), tavo)) : __dsqrt_rn(J2sq);
               f.txyav[j * pitch + i] = tavo;
@@ -164,9 +164,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
             // column pairs: nodes (i, j) + (i, j+1), then (i+1, j) + (i+1, j+1)
             const double sx = pair_sum4(s.xx[lj][li], s.xx[lj + 1][li], s.xx[lj][li + 1], s.xx[lj + 1][li + 1]);
             const double sy = pair_sum4(s.yy[lj][li], s.yy[lj + 1][li], s.yy[lj][li + 1], s.yy[lj + 1][li + 1]);
-            const double J2sq = corner_j2sq(sx, sy, s.xy[lj + 1][li + 1]);
-            fc = return_factor(J2sq, coh, coh2);
-            if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = __dsqrt_rn(J2sq);
+            const double J2sq16 = corner_j2sq16(sx, sy, s.xy[lj + 1][li + 1]);  // 16 J2^2
+            fc = return_factor(J2sq16, coh4, coh2x16);
+            if (RECORD && li >= 1 && lj >= 1) f.j2xy[cj * pitch + ci] = __dmul_rn(0.25, __dsqrt_rn(J2sq16));
           }
           s.fc[lj][li] = fc;
         }
@@ -187,7 +187,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
   }
 
   // ---- D: damped momentum update and U += V dt on the owned faces
-  const double dT = g.dT, cX = g.cX, cY = g.cY, dtr = g.dtr;
+  const double dT = g.dT, cX = g.cX, cY = g.cY, dtrX = g.dtrX, dtrY = g.dtrY;
   double vmx = 0.0, vmy = 0.0;
 #pragma unroll
   for (int r = 0; r < RY; r++) {
@@ -197,8 +197,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
     const size_t q = j * pitch + i;
     double vx = vxr[r];
     if (i > 0 && j > 0 && j < ny - 1) {
-      vx = face_velocity(vx, cX, dtr, face_diff(s.p[lj + 1][li + 1], s.p[lj + 1][li], s.xx[lj + 1][li + 1], s.xx[lj + 1][li]),
-                         rdX, __dsub_rn(s.xy[lj + 2][li + 1], s.xy[lj + 1][li + 1]), rdY);
+      vx = face_velocity_s(vx, cX,
+                           face_diff(s.p[lj + 1][li + 1], s.p[lj + 1][li], s.xx[lj + 1][li + 1], s.xx[lj + 1][li]),
+                           dtrX, __dsub_rn(s.xy[lj + 2][li + 1], s.xy[lj + 1][li + 1]), dtrY);
       const TV vs = (TV)vx;
       fvx[q] = vs;
       vx = (double)vs;  // the displacement moves by the stored velocity
@@ -206,8 +207,9 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
     uxo[q] = advance(s.ux[lj + 2][li + 1], vx, dT);
     double vy = vyr[r];
     if (i > 0 && i < nx - 1 && j > 0) {
-      vy = face_velocity(vy, cY, dtr, face_diff(s.p[lj + 1][li + 1], s.p[lj][li + 1], s.yy[lj + 1][li + 1], s.yy[lj][li + 1]),
-                         rdY, __dsub_rn(s.xy[lj + 1][li + 2], s.xy[lj + 1][li + 1]), rdX);
+      vy = face_velocity_s(vy, cY,
+                           face_diff(s.p[lj + 1][li + 1], s.p[lj][li + 1], s.yy[lj + 1][li + 1], s.yy[lj][li + 1]),
+                           dtrY, __dsub_rn(s.xy[lj + 1][li + 2], s.xy[lj + 1][li + 1]), dtrX);
       const TV vs = (TV)vy;
       fvy[q] = vs;
       vy = (double)vs;

@@ -193,8 +193,8 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
     cp_async_zfill<4>(&row.m[lane], mask + (rm ? ((k * pitch + i) & ~3) : 0), rm);
   };
   const T rdX = (T)g.rdX, rdY = (T)g.rdY, third = (T)(1.0 / 3.0);
-  const T coh = (T)g.coh, coh2 = (T)g.coh2;
-  const T dT = (T)g.dT, cX = (T)g.cX, cY = (T)g.cY, dtr = (T)g.dtr;
+  const T coh = (T)g.coh, coh2 = (T)g.coh2, coh4 = (T)g.coh4, coh2x16 = (T)g.coh2x16;
+  const T dT = (T)g.dT, cX = (T)g.cX, cY = (T)g.cY, dtrX = (T)g.dtrX, dtrY = (T)g.dtrY;
   const T exx0 = (T)g.exx0, eyy0 = (T)g.eyy0, exy0 = (T)g.exy0;  // FP32 bulk only
   __syncwarp();  // the previous segment of this warp has stopped reading the tables
   sm.g4z[lane] = (T)g4z_entry(lane, g.G0, g.Gp);
@@ -307,19 +307,18 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       T xr = xa, yr = ya, cr = c2;
       if (PLASTIC) {
         // node: tauXY averaged from the clamped 2x2 corner block (EffPlast2D.cu:109-135)
-        T tav;
+        T hsum;  // the four-corner sum; tauXY averaged onto the node is hsum / 4
         if (INTERIOR) {  // the block below-left: corners (i-1..i, j-1..j), rows j-1 and j
-          tav = mul_rn((T)0.25, add_rn(hs0, hs1));
+          hsum = add_rn(hs0, hs1);
         } else {
           const int a = min(max(i - 1, 0), nx - 3) - i;  // -2, -1 or 0 inside the grid
           const int bsel = min(max(j - 1, 0), ny - 3) - j;
           const T cr0 = (bsel == 0) ? c2 : (bsel == -1 ? c1 : c0);  // row j + bsel
           const T cr1 = (bsel == 0) ? c3 : (bsel == -1 ? c2 : c1);  // row j + bsel + 1
           const int sa = min(max(lane + a, 0), 31), sb = min(max(lane + a + 1, 0), 31);
-          tav = mul_rn((T)0.25, pair_sum4(shfl_idx(cr0, sa), shfl_idx(cr0, sb), shfl_idx(cr1, sa),
-                                          shfl_idx(cr1, sb)));
+          hsum = pair_sum4(shfl_idx(cr0, sa), shfl_idx(cr0, sb), shfl_idx(cr1, sa), shfl_idx(cr1, sb));
         }
-        const T nJ2sq = node_j2sq(xa, ya, tav);
+        const T nJ2sq = node_j2sq_h(xa, ya, hsum);
         const bool node_in = INTERIOR || (coln && j >= 0 && j < ny);
         const T fn = node_in ? return_factor(nJ2sq, coh, coh2) : (T)1;
         // corner: node deviators (i..i+1, j..j+1) = rows a (j) and b (j+1), summed as
@@ -327,19 +326,19 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         const T vx_ = add_rn(xa, xb), vy_ = add_rn(ya, yb);
         const T sx = add_rn(vx_, shfl_dn(vx_));
         const T sy = add_rn(vy_, shfl_dn(vy_));
-        const T cJ2sq = corner_j2sq(sx, sy, c2);
+        const T cJ2sq16 = corner_j2sq16(sx, sy, c2);  // 16 J2^2
         const bool corner_in = INTERIOR || (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1);
-        const T fc = corner_in ? return_factor(cJ2sq, coh, coh2) : (T)1;
+        const T fc = corner_in ? return_factor(cJ2sq16, coh4, coh2x16) : (T)1;
         if (TRACK) {  // J2 > coh from the trial stresses (get_sigma_2D.m:126-138)
           yld_n = node_in && nJ2sq > coh2;
-          yld_c = corner_in && cJ2sq > coh2;
+          yld_c = corner_in && cJ2sq16 > coh2x16;
         }
         if (REC_STRESS) {
-          tav_o = node_in ? mul_rn(tav, fn) : (T)0;
+          tav_o = node_in ? mul_rn(mul_rn((T)0.25, hsum), fn) : (T)0;
           j2_o = !node_in ? (T)0
                           : (fn != (T)1) ? sqrt_rn(node_j2sq(mul_rn(xa, fn), mul_rn(ya, fn), tav_o))
                                          : sqrt_rn(nJ2sq);
-          j2xy_o = corner_in ? sqrt_rn(cJ2sq) : (T)0;
+          j2xy_o = corner_in ? mul_rn((T)0.25, sqrt_rn(cJ2sq16)) : (T)0;
         }
         xr = mul_rn(xa, fn);
         yr = mul_rn(ya, fn);
@@ -358,8 +357,8 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
       const StreamRow<TU, TV>& rj = sm.ring[s_k2];
       const T uxm = rj.ux[lane], uym = rj.uy[lane];
       const T vxm = (T)rj.vx[lane], vym = (T)rj.vy[lane];
-      const TV vxs = (TV)face_velocity(vxm, cX, dtr, face_diff(pw, pw_l, xw, xw_l), rdX, sub_rn(cw_l, cq_l), rdY);
-      const TV vys = (TV)face_velocity(vym, cY, dtr, face_diff(pw, pq, yw, yq), rdY, sub_rn(cq, cq_l), rdX);
+      const TV vxs = (TV)face_velocity_s(vxm, cX, face_diff(pw, pw_l, xw, xw_l), dtrX, sub_rn(cw_l, cq_l), dtrY);
+      const TV vys = (TV)face_velocity_s(vym, cY, face_diff(pw, pq, yw, yq), dtrY, sub_rn(cq, cq_l), dtrX);
       // the displacement moves by the stored velocity
       const T vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (T)vxs : vxm;
       const T vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (T)vys : vym;

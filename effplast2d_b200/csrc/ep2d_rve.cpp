@@ -400,6 +400,10 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   g.cX = 1.0 - g.dT * g.dampX;
   g.cY = 1.0 - g.dT * g.dampY;
   g.dtr = g.dT / g.rho;
+  g.coh4 = 4.0 * g.coh;
+  g.coh2x16 = g.coh4 * g.coh4;
+  g.dtrX = g.dtr * g.rdX;
+  g.dtrY = g.dtr * g.rdY;
 
   if (s) {
     stream = s;

@@ -6,12 +6,14 @@
 // that calls these functions therefore rounds every cell identically, whatever the
 // surrounding code, the tile or segment shape, or the batch the RVE runs in; results
 // of the kernel forms are equal bit for bit.  The operations follow the reference's
-// expressions (EffPlast2D.cu:37-177) with five rewrites that change rounding only:
-// divisions by dX, dY, 3 and rho are multiplications by host-computed reciprocals, the
-// yield test compares J2^2 with coh^2, the return factor coh / J2 is coh * rsqrt(J2^2)
-// (CUDA's double rsqrt, within 1 ulp; the factor within 2 ulp of the quotient), the
-// four-term sums of the tauXY average and of the corner deviators add two pair sums
-// (pair_sum4) instead of left to right, and the marked products and sums are fused.
+// expressions (EffPlast2D.cu:37-177) with rewrites that change rounding only: divisions
+// by dX, dY, 3 and rho are multiplications by host-computed reciprocals (dt/rho folded
+// into the face factors), the yield test compares J2^2 with coh^2 (16 J2^2 with 16 coh^2
+// at corners), the return factor coh / J2 is coh * rsqrt(J2^2) (CUDA's double rsqrt,
+// within 1 ulp; the factor within 2 ulp of the quotient), the four-term sums of the
+// tauXY average and of the corner deviators add two pair sums (pair_sum4) instead of left
+// to right, the averages' 1/4 is folded into the J2 formulas, and the marked products and
+// sums are fused.
 #pragma once
 
 #include "ep2d_types.hpp"
@@ -50,9 +52,19 @@ __device__ __forceinline__ double node_j2sq(double xx, double yy, double tav) {
   return __fma_rn(xx, xx, __fma_rn(yy, yy, __dmul_rn(2.0, __dmul_rn(tav, tav))));
 }
 
-// J2^2 at a corner from the sums of the four node deviators around it (:137-145).
-__device__ __forceinline__ double corner_j2sq(double sx, double sy, double t) {
-  return __fma_rn(__dmul_rn(0.0625, sx), sx, __fma_rn(__dmul_rn(0.0625, sy), sy, __dmul_rn(2.0, __dmul_rn(t, t))));
+// J2^2 at a node from h = the four-corner tauXY sum (the average is h / 4):
+// xx^2 + yy^2 + 2 (h/4)^2 = xx^2 + yy^2 + 0.125 h^2, two operations fewer than forming
+// the average first.
+__device__ __forceinline__ double node_j2sq_h(double xx, double yy, double h) {
+  return __fma_rn(xx, xx, __fma_rn(yy, yy, __dmul_rn(__dmul_rn(0.125, h), h)));
+}
+
+// 16 J2^2 at a corner from the sums sx, sy of the four node deviators around it
+// (:137-145): sx^2 + sy^2 + 32 t^2 = 16 ((sx/4)^2 + (sy/4)^2 + 2 t^2).  Its
+// yield test compares with 16 coh^2 and its factor is 4 coh rsqrt(16 J2^2) = coh / J2,
+// so the 1/16 is never applied.
+__device__ __forceinline__ double corner_j2sq16(double sx, double sy, double t) {
+  return __fma_rn(sx, sx, __fma_rn(sy, sy, __dmul_rn(__dmul_rn(32.0, t), t)));
 }
 
 // Radial return factor (ComputePlasticity, :147-177): coh / J2 where J2 > coh, else 1.
@@ -60,11 +72,10 @@ __device__ __forceinline__ double return_factor(double j2sq, double coh, double 
   return (j2sq > coh2) ? __dmul_rn(coh, rsqrt(j2sq)) : 1.0;
 }
 
-// ComputeDisp (:3-35): damped momentum update of one face velocity,
-// v (1 - dt damp) + dt/rho (dA rA + dB rB).
-__device__ __forceinline__ double face_velocity(double v, double c, double dtr, double dA, double rA, double dB,
-                                                double rB) {
-  return __fma_rn(v, c, __dmul_rn(dtr, __fma_rn(dA, rA, __dmul_rn(dB, rB))));
+// ComputeDisp (:3-35): damped momentum update of one face velocity with the factors
+// sA = dt/rho rA and sB = dt/rho rB formed on the host: v (1 - dt damp) + dA sA + dB sB.
+__device__ __forceinline__ double face_velocity_s(double v, double c, double dA, double sA, double dB, double sB) {
+  return __fma_rn(v, c, __fma_rn(dA, sA, __dmul_rn(dB, sB)));
 }
 
 // Stress differences of a face: ((-p + p_n) + t) - t_n, in the reference's order.
@@ -99,15 +110,17 @@ __device__ __forceinline__ float corner_trial(float g4, float dxy, float dyx, fl
 __device__ __forceinline__ float node_j2sq(float xx, float yy, float tav) {
   return __fmaf_rn(xx, xx, __fmaf_rn(yy, yy, __fmul_rn(2.0f, __fmul_rn(tav, tav))));
 }
-__device__ __forceinline__ float corner_j2sq(float sx, float sy, float t) {
-  return __fmaf_rn(__fmul_rn(0.0625f, sx), sx,
-                   __fmaf_rn(__fmul_rn(0.0625f, sy), sy, __fmul_rn(2.0f, __fmul_rn(t, t))));
+__device__ __forceinline__ float node_j2sq_h(float xx, float yy, float h) {
+  return __fmaf_rn(xx, xx, __fmaf_rn(yy, yy, __fmul_rn(__fmul_rn(0.125f, h), h)));
+}
+__device__ __forceinline__ float corner_j2sq16(float sx, float sy, float t) {
+  return __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, __fmul_rn(__fmul_rn(32.0f, t), t)));
+}
+__device__ __forceinline__ float face_velocity_s(float v, float c, float dA, float sA, float dB, float sB) {
+  return __fmaf_rn(v, c, __fmaf_rn(dA, sA, __fmul_rn(dB, sB)));
 }
 __device__ __forceinline__ float return_factor(float j2sq, float coh, float coh2) {
   return (j2sq > coh2) ? __fmul_rn(coh, rsqrtf(j2sq)) : 1.0f;
-}
-__device__ __forceinline__ float face_velocity(float v, float c, float dtr, float dA, float rA, float dB, float rB) {
-  return __fmaf_rn(v, c, __fmul_rn(dtr, __fmaf_rn(dA, rA, __fmul_rn(dB, rB))));
 }
 __device__ __forceinline__ float face_diff(float p, float p_n, float t, float t_n) {
   return __fsub_rn(__fadd_rn(__fsub_rn(p_n, p), t), t_n);

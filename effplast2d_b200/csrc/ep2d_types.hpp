@@ -24,6 +24,8 @@ struct Geo {
   // host-computed factors of the iteration kernel: 1/dX, 1/dY, coh^2,
   // 1 - dT dampX, 1 - dT dampY, dT / rho
   double rdX, rdY, coh2, cX, cY, dtr;
+  // 4 coh, 16 coh^2 (the corner return), dt/rho / dX, dt/rho / dY (the face updates)
+  double coh4, coh2x16, dtrX, dtrY;
   // FP32 bulk only: strains of the affine field Ua its displacements are measured from:
   // exx0 = dUa_x/dx, eyy0 = dUa_y/dy, exy0 = dUa_x/dy + dUa_y/dx (= 2 Exy)
   double exx0, eyy0, exy0;
