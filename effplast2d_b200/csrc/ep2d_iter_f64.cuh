@@ -198,7 +198,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
     double vx = vxr[r];
     if (i > 0 && j > 0 && j < ny - 1) {
       vx = face_velocity_s(vx, cX,
-                           face_diff(s.p[lj + 1][li + 1], s.p[lj + 1][li], s.xx[lj + 1][li + 1], s.xx[lj + 1][li]),
+                           stress_diff(s.p[lj + 1][li + 1], s.p[lj + 1][li], s.xx[lj + 1][li + 1], s.xx[lj + 1][li]),
                            dtrX, __dsub_rn(s.xy[lj + 2][li + 1], s.xy[lj + 1][li + 1]), dtrY);
       const TV vs = (TV)vx;
       fvx[q] = vs;
@@ -208,7 +208,7 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
     double vy = vyr[r];
     if (i > 0 && i < nx - 1 && j > 0) {
       vy = face_velocity_s(vy, cY,
-                           face_diff(s.p[lj + 1][li + 1], s.p[lj][li + 1], s.yy[lj + 1][li + 1], s.yy[lj][li + 1]),
+                           stress_diff(s.p[lj + 1][li + 1], s.p[lj][li + 1], s.yy[lj + 1][li + 1], s.yy[lj][li + 1]),
                            dtrY, __dsub_rn(s.xy[lj + 1][li + 2], s.xy[lj + 1][li + 1]), dtrX);
       const TV vs = (TV)vy;
       fvy[q] = vs;

@@ -230,7 +230,9 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
   T c2_l = 0;  // corner trial row r-1 of column i-1; next step: row r-2
   T hs1 = 0;
   // returned stresses: nodes rows r-2 (q) and r-1 (w); corners rows r-2 (cq), r-1 (cw)
-  T pq = 0, yq = 0, pw = 0, xw = 0, yw = 0, cq = 0, cw = 0;
+  T pw = 0, xw = 0, yw = 0, cq = 0, cw = 0;
+  // total normal stresses tau - P of row r-1 (sxw, syw) and syy of row r-2 (syq)
+  T sxw = 0, syw = 0, syq = 0;
   T cw_l = 0;  // returned corner row r-1 of column i-1; next step: row r-2
 
   // slots of rows k, k-1, k-2
@@ -345,20 +347,22 @@ __device__ __forceinline__ void stream_task(const Geo& g, const Fields& f, const
         cr = mul_rn(c2, fc);
       }
       cq_l = cw_l;
-      pq = pw; yq = yw; cq = cw;
+      syq = syw; cq = cw;
       pw = pa_; xw = xr; yw = yr; cw = cr;
+      sxw = sub_rn(xw, pw);
+      syw = sub_rn(yw, pw);
       cw_l = shfl_up1(cw);
     }
 
     // ---- faces of row j (owned rows [jA, jB)); U and V of row j from the ring.  A face
     // the reference leaves alone gets its old velocity back, unchanged.
     if constexpr (STAGE == 2) {
-      const T pw_l = shfl_up1(pw), xw_l = shfl_up1(xw);
+      const T sxw_l = shfl_up1(sxw);
       const StreamRow<TU, TV>& rj = sm.ring[s_k2];
       const T uxm = rj.ux[lane], uym = rj.uy[lane];
       const T vxm = (T)rj.vx[lane], vym = (T)rj.vy[lane];
-      const TV vxs = (TV)face_velocity_s(vxm, cX, face_diff(pw, pw_l, xw, xw_l), dtrX, sub_rn(cw_l, cq_l), dtrY);
-      const TV vys = (TV)face_velocity_s(vym, cY, face_diff(pw, pq, yw, yq), dtrY, sub_rn(cq, cq_l), dtrX);
+      const TV vxs = (TV)face_velocity_s(vxm, cX, sub_rn(sxw, sxw_l), dtrX, sub_rn(cw_l, cq_l), dtrY);
+      const TV vys = (TV)face_velocity_s(vym, cY, sub_rn(syw, syq), dtrY, sub_rn(cq, cq_l), dtrX);
       // the displacement moves by the stored velocity
       const T vx = (INTERIOR || (i > 0 && j > 0 && j < ny - 1)) ? (T)vxs : vxm;
       const T vy = (INTERIOR || (i > 0 && i < nx - 1 && j > 0)) ? (T)vys : vym;

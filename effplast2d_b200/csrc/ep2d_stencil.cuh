@@ -78,9 +78,11 @@ __device__ __forceinline__ double face_velocity_s(double v, double c, double dA,
   return __fma_rn(v, c, __fma_rn(dA, sA, __dmul_rn(dB, sB)));
 }
 
-// Stress differences of a face: ((-p + p_n) + t) - t_n, in the reference's order.
-__device__ __forceinline__ double face_diff(double p, double p_n, double t, double t_n) {
-  return __dsub_rn(__dadd_rn(__dsub_rn(p_n, p), t), t_n);
+// Normal-stress difference across a face, (t - p) - (t_n - p_n): the total stresses
+// tau - P of the two nodes, each formed once per node (the stream form forms it before
+// its one shuffle) and then subtracted.
+__device__ __forceinline__ double stress_diff(double p, double p_n, double t, double t_n) {
+  return __dsub_rn(__dsub_rn(t, p), __dsub_rn(t_n, p_n));
 }
 
 // U += V dt
@@ -122,8 +124,8 @@ __device__ __forceinline__ float face_velocity_s(float v, float c, float dA, flo
 __device__ __forceinline__ float return_factor(float j2sq, float coh, float coh2) {
   return (j2sq > coh2) ? __fmul_rn(coh, rsqrtf(j2sq)) : 1.0f;
 }
-__device__ __forceinline__ float face_diff(float p, float p_n, float t, float t_n) {
-  return __fsub_rn(__fadd_rn(__fsub_rn(p_n, p), t), t_n);
+__device__ __forceinline__ float stress_diff(float p, float p_n, float t, float t_n) {
+  return __fsub_rn(__fsub_rn(t, p), __fsub_rn(t_n, p_n));
 }
 __device__ __forceinline__ float advance(float u, float v, float dT) { return __fmaf_rn(v, dT, u); }
 
