@@ -369,9 +369,11 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   EP2D_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   shape = shape_of(p, sms);
   {
-    ep2d_params ps = p;  // the FP32 bulk always runs the stream form
+    // the FP32 bulk always runs the stream form: the parameters' segment height when they
+    // pin the stream form, else the library's choice for the grid
+    ep2d_params ps = p;
+    if (ps.kernel != EP2D_KERNEL_STREAM) ps.rows = 0;
     ps.kernel = EP2D_KERNEL_STREAM;
-    ps.rows = 0;
     f32_rows = shape_of(ps, sms).rows;
   }
   d = derive(p);
