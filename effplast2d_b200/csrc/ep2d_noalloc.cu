@@ -63,20 +63,22 @@ int scratch_on_current_device(double** out) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(EP2D_ERR_NODEV, std::string("no current CUDA device: ") + cudaGetErrorString(e));
-  // cudaFree(nullptr) makes the device's primary context current without allocating
-  e = cudaFree(nullptr);
-  CUcontext ctx = nullptr;
   CtxGetCurrentFn get = ctx_get_current();
-  if (e != cudaSuccess || !get || get(&ctx) != CUDA_SUCCESS || !ctx)
-    return fail(EP2D_ERR_CUDA, std::string("no current CUDA context for the scratch lookup: ") +
-                                   cudaGetErrorString(e));
+  if (!get) return fail(EP2D_ERR_CUDA, "cuCtxGetCurrent is not available from the CUDA driver");
+  // the context current on this thread; null before the runtime has made one current,
+  // which the lookup below does (cudaGetSymbolAddress initialises the device's primary
+  // context; nothing here allocates)
+  CUcontext ctx = nullptr;
+  if (get(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx) {
+  if (!ctx || !g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_avg_scratch);
     if (e != cudaSuccess || !p)
       return fail(EP2D_ERR_CUDA, std::string("cudaGetSymbolAddress of the averaging scratch: ") +
                                      cudaGetErrorString(e));
+    if (!ctx && (get(&ctx) != CUDA_SUCCESS || !ctx))
+      return fail(EP2D_ERR_CUDA, "no current CUDA context after the scratch lookup");
     g_scratch_dev[dev] = static_cast<double*>(p);
     g_scratch_ctx[dev] = ctx;
   }
