@@ -78,3 +78,27 @@ def test_f32_bulk_rejected_by_batches():
         B.batch_solve([B.spec(64, pa, 2, 1, -6e-5, (1.0, 1.0, 0.0))], niter=2000, check_every=1000,
                       precision=ep.F32_BULK)
     assert e.value.status == ep.ERR_ARG
+
+
+def test_f32_round_trip_keeps_displacements():
+    # zero FP32 iterations: U -> u' = U - Ua (float) -> U = Ua + u' changes U only by the
+    # float rounding of the perturbation, never by the affine part
+    n = 96
+    s = solver(n, ep.F32_BULK, 2000, 1000)
+    s.solve_step(0, -6e-5, [1.0, 0.8, 0.3], 1)
+    before = {f: s.get(f) for f in ("Ux", "Uy")}
+    s.iterate_f32(0)
+    for f in ("Ux", "Uy"):
+        after = s.get(f)
+        # the perturbation is at most |U| here; its float rounding is 2^-24 of it
+        assert np.max(np.abs(after - before[f])) <= 2.0 ** -23 * np.max(np.abs(before[f])), f
+    s.iterate_f32(500)
+    assert s.stats()["f32_iterations"] == 500
+    s.close()
+    with pytest.raises(ep.EP2DError) as e:  # FP64 handles have no FP32 form
+        s64 = solver(n, ep.FP64, 2000, 1000)
+        try:
+            s64.iterate_f32(10)
+        finally:
+            s64.close()
+    assert e.value.status == ep.ERR_STATE
