@@ -48,6 +48,16 @@ WORKLOADS = {
                  n_time_steps=1, nl=3, niter=5_000_000, eiter=1e-9, check_every=10_000,
                  label="2048x2048 grid, 4x4 pores, porosity 0.02, K0=1 G0=0.5 Y=1e-5, preload -6e-5*[1,1,0.5] "
                        "+ bulk and shear increments (NL=3), eIter 1e-9"),
+    # single small RVEs of the batched workload's kind (sides 256 and 512): too small to
+    # fill the GPU, where one iteration is a few microseconds and the launch boundary counts
+    "rve256": dict(n=256, n_pores=2, porosity=0.02, g0=0.5, yield_stress=1e-5, load=-6e-5, load_type=(1.0, 1.0, 0.5),
+                   n_time_steps=1, nl=3, niter=2_000_000, eiter=1e-9, check_every=10_000,
+                   label="256x256 grid, 2x2 pores, porosity 0.02, K0=1 G0=0.5 Y=1e-5, preload -6e-5*[1,1,0.5] "
+                         "+ bulk and shear increments (NL=3), eIter 1e-9"),
+    "rve512": dict(n=512, n_pores=2, porosity=0.02, g0=0.5, yield_stress=1e-5, load=-6e-5, load_type=(1.0, 1.0, 0.5),
+                   n_time_steps=1, nl=3, niter=2_000_000, eiter=1e-9, check_every=10_000,
+                   label="512x512 grid, 2x2 pores, porosity 0.02, K0=1 G0=0.5 Y=1e-5, preload -6e-5*[1,1,0.5] "
+                         "+ bulk and shear increments (NL=3), eIter 1e-9"),
     # the reference's CPU-runnable case (elastic, one pore)
     "cfg1": dict(n=128, n_pores=1, porosity=0.005, g0=0.5, yield_stress=1.0, load=-4e-5, load_type=(1.0, 1.0, 0.0),
                  n_time_steps=1, nl=1, niter=100_000, eiter=1e-9, check_every=10_000,
@@ -399,7 +409,7 @@ def run_ours(args, w):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": bench_config(w, args.workload, world, ips),
-            "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
+            "kernel": {"form": KERNEL_NAMES[shape[0]], "rows": shape[1]},
             "e2e": None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
@@ -448,7 +458,7 @@ def run_ours(args, w):
     return 0
 
 
-def kernel_timing(workload, iters, kernel=0, rows=0, precision="fp64"):
+def kernel_timing(workload, iters, kernel=0, rows=0, precision="fp64", w=None):
     """Exactly `iters` pseudo-time iterations of the workload's preload step (no
     convergence test), after one untimed pass of the same length: CUDA-event time per
     launch of the fused iteration kernel on its own stream, and its HBM roofline.
@@ -457,7 +467,7 @@ def kernel_timing(workload, iters, kernel=0, rows=0, precision="fp64"):
 
     import effplast2d_b200 as ep
 
-    w = WORKLOADS[workload]
+    w = w or WORKLOADS[workload]
     n = w["n"]
     prec = {"fp64": ep.FP64, "mixed": ep.MIXED, "f32": ep.F32_BULK}[precision]
     s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=iters, eiter=0.0, check_every=iters, device=0,
@@ -477,21 +487,49 @@ def kernel_timing(workload, iters, kernel=0, rows=0, precision="fp64"):
     st1 = s.stats()
     shape = s.kernel_shape()
     s.close()
-    per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(st1["launches"] - st0["launches"], 1)
+    # per iteration (a resident-form launch runs many)
+    iters_run = (st1["cell_updates"] - st0["cell_updates"]) // (n * n)
+    per = (st1["kernel_ms"] - st0["kernel_ms"]) / max(iters_run, 1)
     bytes_alg = {"fp64": 64, "mixed": 48, "f32": 32}[precision] * n * n
     peak, kind = measured_peaks()
     achieved = bytes_alg / (per / 1e3) / 1e9
     return {"workload": workload, "grid": "%dx%d" % (n, n), "iterations": iters, "precision": precision,
-            "kernel": {"form": "tile" if shape[0] == ep.KERNEL_TILE else "stream", "rows": shape[1]},
+            "kernel": {"form": KERNEL_NAMES[shape[0]], "rows": shape[1]},
+            "iteration_launches": st1["launches"] - st0["launches"],
             "avg_launch_us": per * 1e3, "algorithmic_bytes_per_launch": bytes_alg, "achieved": achieved,
             "peak": peak, "unit": "GB/s", "peak_source": kind, "frac": achieved / peak,
             "traffic": ncu_traffic(workload), "wall_s": wall, "cell_updates_per_s": n * n / (per / 1e3)}
 
 
+KERNEL_NAMES = {0: "auto", 1: "tile", 2: "stream", 3: "resident"}
+
+
+def run_solve_only(args, w):
+    """One complete ComputeEffModuli solve of the workload with the chosen kernel form:
+    device time, iterations, time per iteration and the moduli."""
+    import effplast2d_b200 as ep
+
+    n = w["n"]
+    s = ep.Solver(n, n, make_pa(w), nl=w["nl"], niter=w["niter"], eiter=w["eiter"], check_every=w["check_every"],
+                  device=0, kernel=args.kernel, rows=args.rows)
+    shape = s.kernel_shape()
+    t = time.perf_counter()
+    r = s.compute_eff_moduli(w["load"], list(w["load_type"]), w["n_time_steps"])
+    wall = time.perf_counter() - t
+    st = s.stats()
+    s.close()
+    iters = st["cell_updates"] // (n * n)
+    print(json.dumps({"workload": args.workload, "kernel": {"form": KERNEL_NAMES[shape[0]], "rows": shape[1]},
+                      "wall_s": wall, "kernel_ms": st["kernel_ms"], "iterations": iters,
+                      "iteration_launches": st["launches"], "us_per_iteration": st["kernel_ms"] * 1e3 / max(iters, 1),
+                      "all_converged": bool(r["all_converged"]), "num": r["num"]}))
+    return 0
+
+
 def run_kernel_only(args, w):
     """The fixed, short launch sequence used for ncu captures and for timing the fused
     iteration kernel alone."""
-    print(json.dumps(kernel_timing(args.workload, args.kernel_only, args.kernel, args.rows, args.precision)))
+    print(json.dumps(kernel_timing(args.workload, args.kernel_only, args.kernel, args.rows, args.precision, w)))
     return 0
 
 
@@ -712,9 +750,13 @@ def main():
     ap.add_argument("--niter", type=int, default=2_000_000, help="NITER of the batch / serve workloads")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="N",
                     help="run N iterations of the workload's preload step and report the kernel timing")
-    ap.add_argument("--kernel", type=int, default=0, choices=[0, 1, 2],
-                    help="iteration kernel form: 0 library's choice, 1 tile, 2 stream")
+    ap.add_argument("--kernel", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="iteration kernel form: 0 library's choice, 1 tile, 2 stream, 3 resident")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="one complete solve of the workload with --kernel/--rows: time per iteration, moduli")
     ap.add_argument("--rows", type=int, default=0, help="rows per tile / strip segment (0: library's choice)")
+    ap.add_argument("--side", type=int, default=0,
+                    help="grid side of --kernel-only / --solve-only (0: the workload's own)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
@@ -749,8 +791,12 @@ def main():
     if args.workload == "serve":
         return run_serve(args)
     w = WORKLOADS[args.workload]
+    if args.side and (args.kernel_only or args.solve_only):
+        w = dict(w, n=args.side)
     if args.kernel_only:
         return run_kernel_only(args, w)
+    if args.solve_only:
+        return run_solve_only(args, w)
     if args.impl == "reference":
         return run_reference(args, w)
     return run_ours(args, w)

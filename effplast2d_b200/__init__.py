@@ -5,8 +5,8 @@ its own entry points: the C ABI of include/ep2d.h (libep2d.so), the drop-in C++
 `EffPlast2D` class and CLI (csrc/dropin), and this Python binding.
 """
 from ._abi import (ERR_ARG, ERR_CUDA, ERR_IO, ERR_NODEV, ERR_NOMEM, ERR_RANGE, ERR_STATE, F32_BULK, FIELDS, FP64,  # noqa: F401
-                   KERNEL_AUTO, KERNEL_STREAM, KERNEL_TILE, MIXED, field_dims)
-from .solver import (EP2DError, Solver, device_count, lib, make_pa, read_pa,  # noqa: F401
-                     write_pa)
+                   KERNEL_AUTO, KERNEL_RESIDENT, KERNEL_STREAM, KERNEL_TILE, MIXED, field_dims)
+from .solver import (EP2DError, Solver, check_grid_barrier, device_count, lib, make_pa,  # noqa: F401
+                     read_pa, write_pa)
 
 __version__ = "0.1.0"

@@ -28,6 +28,7 @@ F32_BULK = 2
 KERNEL_AUTO = 0
 KERNEL_TILE = 1
 KERNEL_STREAM = 2
+KERNEL_RESIDENT = 3
 
 # field identifiers (include/ep2d.h), in the reference's array order
 FIELDS = ("P", "tauXX", "tauYY", "tauXY", "tauXYav", "J2", "J2XY",

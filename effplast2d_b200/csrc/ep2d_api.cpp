@@ -234,8 +234,34 @@ int ep2d_polar_fields(ep2d_handle* h, double load_value, double* snu_rr, double*
 
 int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows) {
   if (!h) return fail(EP2D_ERR_ARG, "null handle");
-  if (kernel) *kernel = h->rve.shape.form == ep2d::FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;
+  if (kernel)
+    *kernel = h->rve.shape.form == ep2d::FORM_TILE       ? EP2D_KERNEL_TILE
+              : h->rve.shape.form == ep2d::FORM_RESIDENT ? EP2D_KERNEL_RESIDENT
+                                                         : EP2D_KERNEL_STREAM;
   if (rows) *rows = h->rve.shape.rows;
+  return EP2D_OK;
+}
+
+int ep2d_check_grid_barrier(int32_t device, int32_t blocks, int32_t missing, int32_t rounds, int64_t timeout_ns,
+                            int32_t* passed, int32_t* flag) {
+  if (!passed || !flag) return fail(EP2D_ERR_ARG, "null argument");
+  if (blocks < 1 || missing < 0 || missing > blocks || rounds < 0 || timeout_ns < 0)
+    return fail(EP2D_ERR_ARG, "need 1 <= blocks, 0 <= missing <= blocks, rounds >= 0, timeout_ns >= 0");
+  if (timeout_ns > 10000000000LL) return fail(EP2D_ERR_ARG, "timeout_ns above 10 s");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EP2D_ERR_NODEV, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");
+  ep2d::DeviceScope ds(device);
+  unsigned* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, 8 * sizeof(unsigned));
+  if (e != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  unsigned hv[3] = {};
+  e = ep2d::launch_grid_barrier_check(d, blocks, missing, rounds, (unsigned long long)timeout_ns, d + 4, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(hv, d + 2, sizeof(hv), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(EP2D_ERR_CUDA, std::string("grid barrier check: ") + cudaGetErrorString(e));
+  *flag = (int32_t)hv[0];    // gbar[2]
+  *passed = (int32_t)hv[2];  // out[0]
   return EP2D_OK;
 }
 

@@ -47,6 +47,8 @@ int validate_config(const ep2d_batch_config& c) {
     return fail(EP2D_ERR_ARG, "the FP32 bulk (EP2D_F32_BULK) runs on single-RVE handles only; batches take EP2D_FP64 "
                               "or EP2D_MIXED");
   if (c.precision != EP2D_FP64 && c.precision != EP2D_MIXED) return fail(EP2D_ERR_ARG, "unknown precision");
+  if (c.kernel == EP2D_KERNEL_RESIDENT)
+    return fail(EP2D_ERR_ARG, "the resident form (EP2D_KERNEL_RESIDENT) runs on single-RVE handles only");
   if (c.kernel < EP2D_KERNEL_AUTO || c.kernel > EP2D_KERNEL_STREAM) return fail(EP2D_ERR_ARG, "unknown kernel form");
   if (c.rows != 0) {
     IterShape sh;

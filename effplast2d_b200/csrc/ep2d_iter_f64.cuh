@@ -49,7 +49,16 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int TX, int TY, bool PLASTIC, bool RECORD, typename TV>
+// Loads of U and V.  COH (the resident form, whose grid writes the arrays it reads in
+// later iterations): through L2 only (ld.global.cg), never from an SM's L1 or the
+// read-only path, which do not see other SMs' stores.
+template <bool COH, typename T>
+__device__ __forceinline__ T ld_field(const T* p) {
+  if constexpr (COH) return __ldcg(p);
+  else return *p;
+}
+
+template <int TX, int TY, bool PLASTIC, bool RECORD, typename TV, bool COH = false>
 __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const int src, const int bx, const int by,
                                           TileSmem<TX, TY>& s) {
   static_assert(TX == 32 && TY % 8 == 0, "the thread mapping assumes 32 x 8 threads and TX == 32");
@@ -74,8 +83,8 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
   for (int r = 0; r < RY; r++) {
     const int i = i0 + tx, j = j0 + ty + 8 * r;
     const bool ok = (i < nx && j < ny);
-    vxr[r] = ok ? (double)fvx[j * pitch + i] : 0.0;
-    vyr[r] = ok ? (double)fvy[j * pitch + i] : 0.0;
+    vxr[r] = ok ? (double)ld_field<COH>(fvx + j * pitch + i) : 0.0;
+    vyr[r] = ok ? (double)ld_field<COH>(fvy + j * pitch + i) : 0.0;
   }
 
   // ---- A: stage Ux (i in [i0-1, i0+TX+1], j in [j0-2, j0+TY]), Uy (i in [i0-2, i0+TX],
@@ -85,10 +94,10 @@ __device__ __forceinline__ void iter_tile(const Geo& g, const Fields& f, const i
 #pragma unroll
     for (int li = tx; li < UW; li += 32) {
       int i = i0 - 1 + li, j = j0 - 2 + lj;
-      s.ux[lj][li] = (i >= 0 && i <= nx && j >= 0 && j < ny) ? ux[j * pitch + i] : 0.0;
+      s.ux[lj][li] = (i >= 0 && i <= nx && j >= 0 && j < ny) ? ld_field<COH>(ux + j * pitch + i) : 0.0;
       i = i0 - 2 + li;
       j = j0 - 1 + lj;
-      s.uy[lj][li] = (i >= 0 && i < nx && j >= 0 && j <= ny) ? uy[j * pitch + i] : 0.0;
+      s.uy[lj][li] = (i >= 0 && i < nx && j >= 0 && j <= ny) ? ld_field<COH>(uy + j * pitch + i) : 0.0;
       j = j0 - 2 + lj;
       s.m[lj][li] = (i >= 0 && i < nx && j >= 0 && j < ny) ? f.mask[j * pitch + i] : (uint8_t)0;
     }
@@ -272,6 +281,108 @@ __global__ void __launch_bounds__(256) k_iter_batch(const BatchEntry* __restrict
     else iter_tile<TX, TY, false, RECORD, TV>(e.g, e.f, src, tc.y & 0xffff, tc.y >> 16, s);
     __syncthreads();  // shared memory is reused by the next tile
   }
+}
+
+// ---- resident form: many iterations per launch ---------------------------------------
+// The reference launches its four kernels once per iteration with a device-wide sync
+// after each (EffPlast2D.cu:389-399); the per-launch forms fuse them into one launch per
+// iteration.  On grids too small to fill the GPU (a few hundred cells per SM) an
+// iteration is a few microseconds of work, and the launch boundary is a large part of
+// it.  The resident form runs all the iterations between two checkpoints in ONE
+// cooperative launch: every CTA stays resident, owns fixed tiles, and after each
+// iteration meets the others at a grid-wide barrier (the iteration's U is then complete
+// and visible, and the next one reads it).  Per tile it runs iter_tile, so its results
+// equal the tile form's bit for bit.
+//
+// The barrier lives in device memory (`Fields::gbar`): gbar[0..1] is a 64-bit count of
+// arrivals, zeroed by the host before each launch; gbar[2] is an error flag, zero when
+// the RVE is created and never cleared.  Barrier k (k = 1, 2, ...) of a launch is passed
+// once the count reaches k x gridDim.x: each CTA adds 1 with release semantics after
+// its threads' stores (a CTA barrier first) and one thread polls the count with acquire
+// semantics (a CTA barrier after), the pattern of a semaphore between CTAs; the count
+// is never reset within a launch, so there is no generation to track.  Every wait is
+// bounded: a CTA that waits longer than timeout_ns sets the flag and returns, and a CTA
+// that sees the flag returns too, so a barrier that cannot complete ends the launch with
+// the flag set instead of hanging.  The flag stays set (later launches return at their
+// first barrier); the host reads it at every checkpoint and reports the RVE as failed.
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// true once the arrival count reaches `target`; false if the wait ran out or another
+// CTA's did
+__device__ __forceinline__ bool grid_barrier(unsigned* gbar, unsigned long long target,
+                                             unsigned long long timeout_ns, int* s_ok) {
+  __syncthreads();  // the CTA's stores of this iteration are issued
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(gbar);
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(cnt) : "memory");
+    int ok = 1;
+    if (ld_acquire_u64(cnt) < target) {
+      const unsigned long long t0 = global_ns();
+      for (;;) {
+        __nanosleep(32);
+        if (ld_acquire_u64(cnt) >= target) break;
+        if (*reinterpret_cast<volatile unsigned*>(gbar + 2)) {
+          ok = 0;
+          break;
+        }
+        if (global_ns() - t0 > timeout_ns) {
+          atomicExch(&gbar[2], 1u);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();  // the other CTAs' stores are visible to this CTA's later loads
+  return *s_ok != 0;
+}
+
+// n_iter plain iterations (no recording) of one RVE, starting from buffer src0.  The
+// grid is 1-D and co-resident (cooperative launch); CTA b owns tiles b, b + grid, ...
+template <int TX, int TY, bool PLASTIC, typename TV>
+__global__ void __launch_bounds__(256) k_iter_resident(Geo g, Fields f, int src0, int n_iter,
+                                                       unsigned long long timeout_ns) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_ok;
+  TileSmem<TX, TY>& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
+  const int ntx = (g.nx + TX - 1) / TX, nty = (g.ny + TY - 1) / TY;
+  const int ntiles = ntx * nty;
+  if (*reinterpret_cast<volatile unsigned*>(f.gbar + 2)) return;  // an earlier launch failed
+  for (int it = 0; it < n_iter; it++) {
+    const int src = src0 ^ (it & 1);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      iter_tile<TX, TY, PLASTIC, false, TV, true>(g, f, src, t % ntx, t / ntx, s);
+      __syncthreads();  // shared memory is reused by the next tile
+    }
+    if (it + 1 < n_iter &&
+        !grid_barrier(f.gbar, (unsigned long long)(it + 1) * gridDim.x, timeout_ns, &s_ok))
+      return;
+  }
+}
+
+// The barrier alone, for the host's check of its failure path: `missing` of the grid's
+// CTAs never arrive (they return at once), so with missing > 0 the others' waits run
+// out after timeout_ns and the flag is set; with missing == 0 every round completes.
+// out[0] = CTAs that passed all rounds.
+__global__ void k_grid_barrier_check(unsigned* gbar, int missing, int rounds, unsigned long long timeout_ns,
+                                     unsigned* out) {
+  __shared__ int s_ok;
+  if ((int)blockIdx.x < missing) return;
+  for (int r = 0; r < rounds; r++)
+    if (!grid_barrier(gbar, (unsigned long long)(r + 1) * gridDim.x, timeout_ns, &s_ok)) return;
+  if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(out, 1u);
 }
 
 }  // namespace ep2d

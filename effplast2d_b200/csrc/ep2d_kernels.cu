@@ -1,5 +1,6 @@
 // ep2d_kernels.cu -- launch wrappers for the sm_100a kernels of ep2d_device.cuh,
 // ep2d_iter_f64.cuh (tile form) and ep2d_iter_stream.cuh (stream form).
+#include <algorithm>
 #include <type_traits>
 
 #include "ep2d_device.cuh"
@@ -28,9 +29,17 @@ cudaError_t set_batch_attr() {
                               (int)smem_bytes<TY>());
 }
 
+template <int TY, bool PLASTIC, typename TV>
+cudaError_t set_resident_attr() {
+  return cudaFuncSetAttribute(k_iter_resident<TILE_X, TY, PLASTIC, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes<TY>());
+}
+
 template <int TY, typename TV>
 cudaError_t set_attrs_ty() {
   cudaError_t e;
+  if ((e = set_resident_attr<TY, false, TV>()) != cudaSuccess) return e;
+  if ((e = set_resident_attr<TY, true, TV>()) != cudaSuccess) return e;
   if ((e = set_one_attr<TY, false, false, TV>()) != cudaSuccess) return e;
   if ((e = set_one_attr<TY, false, true, TV>()) != cudaSuccess) return e;
   if ((e = set_one_attr<TY, true, false, TV>()) != cudaSuccess) return e;
@@ -62,6 +71,39 @@ cudaError_t launch_batch_ty(const BatchEntry* ents, const int2* tiles, const int
   if (record) k_iter_batch<TILE_X, TY, true, TV><<<blocks, block, sm, stream>>>(ents, tiles, ntiles, parity);
   else k_iter_batch<TILE_X, TY, false, TV><<<blocks, block, sm, stream>>>(ents, tiles, ntiles, parity);
   return cudaGetLastError();
+}
+
+// One cooperative launch of the resident form: as many CTAs as there are tiles, at most
+// as many as fit on the GPU at once (the barrier needs all of them resident).
+template <int TY, bool PLASTIC, typename TV>
+cudaError_t launch_resident_ty(const Geo& g, const Fields& f, int src, int n_iter, unsigned long long timeout_ns,
+                               cudaStream_t stream) {
+  auto kern = k_iter_resident<TILE_X, TY, PLASTIC, TV>;
+  const size_t sm = smem_bytes<TY>();
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+  const int64_t ntiles = (int64_t)((g.nx + TILE_X - 1) / TILE_X) * ((g.ny + TY - 1) / TY);
+  const int blocks = (int)std::min<int64_t>(ntiles, (int64_t)per_sm * sms);
+  // the arrival count starts at zero; the error flag (gbar[2]) is left as it is
+  if ((e = cudaMemsetAsync(f.gbar, 0, 2 * sizeof(unsigned), stream)) != cudaSuccess) return e;
+  Geo ga = g;
+  Fields fa = f;
+  int srca = src, na = n_iter;
+  unsigned long long to = timeout_ns;
+  void* args[] = {&ga, &fa, &srca, &na, &to};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(blocks), dim3(kIterThreadsX, kIterThreadsY),
+                                     args, sm, stream);
+}
+
+template <int TY, typename TV>
+cudaError_t launch_resident_tv(const Geo& g, const Fields& f, int src, bool plastic, int n_iter,
+                               unsigned long long timeout_ns, cudaStream_t stream) {
+  return plastic ? launch_resident_ty<TY, true, TV>(g, f, src, n_iter, timeout_ns, stream)
+                 : launch_resident_ty<TY, false, TV>(g, f, src, n_iter, timeout_ns, stream);
 }
 
 template <int TY, typename TV>
@@ -176,6 +218,46 @@ cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bo
   if (tile_y == 8) return launch_iter_ty<8, double>(g, f, src, plastic, record, stream);
   if (tile_y == 32) return launch_iter_ty<32, double>(g, f, src, plastic, record, stream);
   return launch_iter_ty<16, double>(g, f, src, plastic, record, stream);
+}
+
+cudaError_t launch_iter_resident(const Geo& g, const Fields& f, int src, bool plastic, bool mixed, int rows,
+                                 int64_t n_iter, unsigned long long timeout_ns, cudaStream_t stream) {
+  if (rows != 8 && rows != 16 && rows != 32) return cudaErrorInvalidValue;
+  if (!f.gbar) return cudaErrorInvalidValue;
+  // in chunks of an even number of iterations below 2^31 (a chunk keeps the parity)
+  constexpr int64_t kChunk = (int64_t)1 << 30;
+  while (n_iter > 0) {
+    const int n = (int)std::min(n_iter, kChunk);
+    cudaError_t e;
+    if (mixed) {
+      e = rows == 8    ? launch_resident_tv<8, float>(g, f, src, plastic, n, timeout_ns, stream)
+          : rows == 32 ? launch_resident_tv<32, float>(g, f, src, plastic, n, timeout_ns, stream)
+                       : launch_resident_tv<16, float>(g, f, src, plastic, n, timeout_ns, stream);
+    } else {
+      e = rows == 8    ? launch_resident_tv<8, double>(g, f, src, plastic, n, timeout_ns, stream)
+          : rows == 32 ? launch_resident_tv<32, double>(g, f, src, plastic, n, timeout_ns, stream)
+                       : launch_resident_tv<16, double>(g, f, src, plastic, n, timeout_ns, stream);
+    }
+    if (e != cudaSuccess) return e;
+    n_iter -= n;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_grid_barrier_check(unsigned* gbar, int blocks, int missing, int rounds,
+                                      unsigned long long timeout_ns, unsigned* out, cudaStream_t stream) {
+  if (blocks < 1 || missing < 0 || missing > blocks || rounds < 0) return cudaErrorInvalidValue;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_barrier_check, 32, 0);
+  if (e != cudaSuccess) return e;
+  if ((int64_t)blocks > (int64_t)per_sm * sms) return cudaErrorCooperativeLaunchTooLarge;
+  if ((e = cudaMemsetAsync(gbar, 0, 4 * sizeof(unsigned), stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(out, 0, sizeof(unsigned), stream)) != cudaSuccess) return e;
+  void* args[] = {&gbar, &missing, &rounds, &timeout_ns, &out};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_grid_barrier_check), dim3(blocks), dim3(32), args,
+                                     0, stream);
 }
 
 cudaError_t launch_iter_f32(const Geo& g, const Fields& f, int src, bool plastic, bool record, int seg_h,

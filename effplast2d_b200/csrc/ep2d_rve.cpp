@@ -77,26 +77,32 @@ int validate_params(const ep2d_params& p) {
   if (!(p.pa[5] > 0.0)) return fail(EP2D_ERR_ARG, "rho0 must be positive");
   if (!(p.pa[10] >= 1.0) || p.pa[10] > 64.0) return fail(EP2D_ERR_ARG, "N (pores per side) must be in [1, 64]");
   if (!(p.pa[9] >= 0.0)) return fail(EP2D_ERR_ARG, "rad must be >= 0");
-  if (p.kernel < EP2D_KERNEL_AUTO || p.kernel > EP2D_KERNEL_STREAM) return fail(EP2D_ERR_ARG, "unknown kernel form");
+  if (p.kernel < EP2D_KERNEL_AUTO || p.kernel > EP2D_KERNEL_RESIDENT) return fail(EP2D_ERR_ARG, "unknown kernel form");
   if (p.rows != 0 && !shape_valid(shape_of(p)))
-    return fail(EP2D_ERR_ARG, "rows must be 8, 16 or 32 for the tile form and 16..1024 for the stream form");
+    return fail(EP2D_ERR_ARG,
+                "rows must be 8, 16 or 32 for the tile and resident forms and 16..1024 for the stream form");
   return EP2D_OK;
 }
 
 IterShape shape_of(const ep2d_params& p, int sm_count) {
   IterShape s;
-  s.form = p.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
-  s.rows = p.rows ? p.rows : (s.form == FORM_TILE ? TILE_Y : SEG_DEFAULT);
+  s.form = p.kernel == EP2D_KERNEL_TILE       ? FORM_TILE
+           : p.kernel == EP2D_KERNEL_RESIDENT ? FORM_RESIDENT
+                                              : FORM_STREAM;
+  s.rows = p.rows ? p.rows : (s.form == FORM_STREAM ? SEG_DEFAULT : TILE_Y);
   if (p.rows == 0 && s.form == FORM_STREAM && sm_count > 0) {
     const int64_t strips = (p.nx + STREAM_COLS - 1) / STREAM_COLS;
     s.rows = 64;
     while (s.rows > SEG_MIN && strips * ((p.ny + s.rows - 1) / s.rows) < 16 * (int64_t)sm_count) s.rows /= 2;
     // too few segments to keep 6 warps on every SM (grids up to ~600^2): a warp's march
     // latency then sets the iteration time, and the tile form, one thread per cell, is
-    // faster (256^2: 7 vs 14 us; 512^2: 10 vs 15 us).  Both forms round alike.
+    // faster (256^2: 7 vs 14 us; 512^2: 10 vs 15 us).  Both forms round alike.  Tiles
+    // of 8 rows where 16-row tiles would give fewer than two per SM (grids up to ~300^2:
+    // 128^2 4.4 vs 5.2 us, 256^2 5.8 vs 7.2 us; 512^2 keeps 16 rows, 10.8 vs 12.1 us).
     if (p.kernel == EP2D_KERNEL_AUTO && strips * ((p.ny + SEG_MIN - 1) / SEG_MIN) < 6 * (int64_t)sm_count) {
       s.form = FORM_TILE;
-      s.rows = TILE_Y;
+      const int64_t tiles16 = (int64_t)((p.nx + TILE_X - 1) / TILE_X) * ((p.ny + TILE_Y - 1) / TILE_Y);
+      s.rows = tiles16 < 2 * (int64_t)sm_count ? 8 : TILE_Y;
     }
   }
   return s;
@@ -319,7 +325,7 @@ size_t Rve::footprint(const ep2d_params& p) {
   if (p.precision == EP2D_F32_BULK) b += 4 * align256(fe * sizeof(float));  // u' (ping-pong)
   b += align256(fe);                                     // mask
   b += align256(partial_elems(p) * sizeof(double));      // averaging partials
-  b += align256((2 * NAVG + n_samples(p) + 2) * sizeof(double));  // sums, samples, vmax
+  b += align256((2 * NAVG + n_samples(p) + 4) * sizeof(double));  // sums, samples, vmax, barrier
   b += align256(n_samples(p) * sizeof(unsigned long long));
   return b;
 }
@@ -457,7 +463,8 @@ int Rve::create(const ep2d_params& p, cudaStream_t s) {
   cp += align256(partial_elems(p) * sizeof(double));
   d_out = reinterpret_cast<double*>(cp);
   f.vmax = reinterpret_cast<unsigned long long*>(d_out + 2 * NAVG + holes.size());
-  cp += align256((2 * NAVG + n_samples(p) + 2) * sizeof(double));
+  f.gbar = reinterpret_cast<unsigned*>(d_out + 2 * NAVG + holes.size() + 2);  // zeroed above, never reset
+  cp += align256((2 * NAVG + n_samples(p) + 4) * sizeof(double));
   d_idx = reinterpret_cast<unsigned long long*>(cp);
 
   EP2D_CK(cudaMallocHost(&h_pin, (2 * NAVG + holes.size() + 2) * sizeof(double) + 64));
@@ -583,6 +590,16 @@ int Rve::capture(int parity) {
 }
 
 int Rve::run_plain(int64_t n) {
+  if (shape.form == FORM_RESIDENT && !f32 && !track) {
+    // one cooperative launch for all n iterations (n == 1: an ordinary tile launch)
+    if (n > 1) {
+      EP2D_CK(launch_iter_resident(g, f, cur, prm.nl > 1, mixed(), shape.rows, n, RESIDENT_TIMEOUT_NS, stream));
+      cur ^= (int)(n & 1);
+      launches++;
+      resident_launches++;
+      return EP2D_OK;
+    }
+  }
   if (n >= kGraphLen) {
     cudaGraphExec_t* ge = f32 ? gexec32_ : gexec_;
     if (!ge[cur]) {
@@ -627,7 +644,7 @@ int Rve::iterate(int64_t n, bool record_last) {
   EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
   kernel_ms += ms;
   cell_updates += n * (int64_t)prm.nx * prm.ny;
-  return EP2D_OK;
+  return check_resident();
 }
 
 double Rve::error_from_vmax(double vmx, double vmy) const {
@@ -637,10 +654,27 @@ double Rve::error_from_vmax(double vmx, double vmy) const {
   return (vmx / (d.dX * (prm.nx - 1)) + vmy / (d.dY * (prm.ny - 1))) * d.dT / std::max(a, b);
 }
 
+// The resident form's barrier error flag (sticky), read back; EP2D_OK if the RVE never
+// ran that form.
+int Rve::check_resident() {
+  if (!resident_launches) return EP2D_OK;
+  unsigned* hf = reinterpret_cast<unsigned*>(h_pin + 2 * NAVG + holes.size() + 2);
+  EP2D_CK(cudaMemcpyAsync(hf, f.gbar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+  EP2D_CK(cudaStreamSynchronize(stream));
+  if (*hf)
+    return fail(EP2D_ERR_CUDA,
+                "resident form: a grid barrier wait ran out (a CTA did not arrive); the RVE's state is invalid");
+  return EP2D_OK;
+}
+
 int Rve::read_error(double* error) {
   unsigned long long* hv = reinterpret_cast<unsigned long long*>(h_pin + 2 * NAVG + holes.size());
   EP2D_CK(cudaMemcpyAsync(hv, f.vmax, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
   EP2D_CK(cudaStreamSynchronize(stream));
+  {
+    const int rc = check_resident();
+    if (rc) return rc;
+  }
   double vmx, vmy;
   std::memcpy(&vmx, &hv[0], sizeof(double));
   std::memcpy(&vmy, &hv[1], sizeof(double));
@@ -813,6 +847,8 @@ int Rve::solve_step(int step, double lsv, const double lt[3], int n_time_steps) 
     EP2D_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     kernel_ms += ms;
     cell_updates += iters * (int64_t)prm.nx * prm.ny;
+    rc = check_resident();  // the last interval may end without a checkpoint
+    if (rc) return rc;
     r.iterations = iters;
     r.converged = converged;
     r.error = error;

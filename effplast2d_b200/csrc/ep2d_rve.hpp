@@ -102,6 +102,7 @@ class Rve {
   int iterate(int64_t n, bool record_last);  // n iterations; the last one records stresses
   int launch_one(bool record);                // one iteration kernel (no stats)
   int reset_vmax();
+  int check_resident();  // the resident form's barrier error flag (sticky)
   int read_error(double* error);              // after a recording launch: D2H + error formula
   int finish_time_step(int step, int it);     // averaging etc. into the record
   double error_from_vmax(double vmx, double vmy) const;
@@ -152,7 +153,8 @@ class Rve {
 
   // statistics
   double kernel_ms = 0.0;
-  int64_t launches = 0;      // fused iteration kernel
+  int64_t launches = 0;      // fused iteration kernel (a resident launch counts once)
+  int64_t resident_launches = 0;  // of them, resident-form launches
   int64_t aux_launches = 0;  // preload, averaging, boundary, gather, mask
   int64_t cell_updates = 0;
 

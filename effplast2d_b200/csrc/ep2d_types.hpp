@@ -44,6 +44,8 @@ struct Fields {
   // FP32 bulk only: the displacement perturbations u' = U - Ua (ping-pong), float
   float* ux32[2];
   float* uy32[2];
+  // resident form: the grid barrier {64-bit arrival count, error flag, unused}, 8-byte aligned
+  unsigned* gbar;
 };
 
 // One RVE of a batched launch.
@@ -60,10 +62,13 @@ constexpr int TILE_X = 32;
 constexpr int TILE_Y = 16;
 constexpr int TILE_Y_CHOICES[3] = {8, 16, 32};
 
-// The two forms of the fused iteration kernel: FORM_TILE (CTA per tile, halos in shared
-// memory; rows = tile height) and FORM_STREAM (warp per 28-column strip segment; rows =
-// segment height, SEG_MIN..SEG_MAX).
-enum IterForm { FORM_TILE = 0, FORM_STREAM = 1 };
+// The forms of the fused iteration kernel: FORM_TILE (CTA per tile, halos in shared
+// memory; rows = tile height), FORM_STREAM (warp per 28-column strip segment; rows =
+// segment height, SEG_MIN..SEG_MAX) and FORM_RESIDENT (the tile form's CTAs kept
+// resident across the iterations between two checkpoints, one cooperative launch;
+// rows = tile height; single launches, the recording ones among them, are tile-form
+// launches).
+enum IterForm { FORM_TILE = 0, FORM_STREAM = 1, FORM_RESIDENT = 2 };
 constexpr int STREAM_COLS = 28;  // columns a warp of the stream form owns (32 lanes, 2-lane halos)
 constexpr int SEG_MIN = 16, SEG_MAX = 1024;
 constexpr int SEG_DEFAULT = 64;
@@ -74,7 +79,7 @@ struct IterShape {
 };
 // true if `s` names a launchable kernel
 inline bool shape_valid(const IterShape& s) {
-  if (s.form == FORM_TILE) return s.rows == 8 || s.rows == 16 || s.rows == 32;
+  if (s.form == FORM_TILE || s.form == FORM_RESIDENT) return s.rows == 8 || s.rows == 16 || s.rows == 32;
   return s.form == FORM_STREAM && s.rows >= SEG_MIN && s.rows <= SEG_MAX;
 }
 // work units of one RVE: tiles or strip segments, as (x, y) counts
@@ -92,6 +97,17 @@ cudaError_t launch_preload(const Geo& g, const Fields& f, int src, double dUxdx,
 // nodes and corners that yield (M_YN, M_YC; stream form and plastic iterations only)
 cudaError_t launch_iter(const Geo& g, const Fields& f, int src, bool plastic, bool record, bool mixed,
                         const IterShape& shape, cudaStream_t stream, bool track = false);
+// n_iter plain iterations of one RVE from buffer src in one cooperative launch (the
+// resident form; tile height `rows`); each barrier wait gives up after timeout_ns,
+// which leaves the error flag f.gbar[2] set (zero when the RVE is created; a set flag
+// makes later launches return at once)
+cudaError_t launch_iter_resident(const Geo& g, const Fields& f, int src, bool plastic, bool mixed, int rows,
+                                 int64_t n_iter, unsigned long long timeout_ns, cudaStream_t stream);
+constexpr unsigned long long RESIDENT_TIMEOUT_NS = 2000000000ull;  // 2 s per barrier wait
+// the grid barrier alone on `blocks` co-resident CTAs, `missing` of which never arrive;
+// out[0] = CTAs that passed all `rounds`; gbar (4 words) zeroed first
+cudaError_t launch_grid_barrier_check(unsigned* gbar, int blocks, int missing, int rounds,
+                                      unsigned long long timeout_ns, unsigned* out, cudaStream_t stream);
 // clear the M_YN / M_YC bits of every node
 cudaError_t launch_clear_track(const Geo& g, uint8_t* mask, cudaStream_t stream);
 // one iteration of the FP32 bulk (stream form, segments of seg_h rows): u' and V in

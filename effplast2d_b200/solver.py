@@ -25,7 +25,7 @@ EXPORTS = (
     "ep2d_batch_solve", "ep2d_rve_footprint", "ep2d_server_create", "ep2d_server_submit", "ep2d_server_wait",
     "ep2d_server_stats", "ep2d_server_destroy", "ep2d_average_fields_noalloc", "ep2d_get_kernel_shape",
     "ep2d_compute_eff_damping", "ep2d_polar_fields", "ep2d_get_f32_iterations",
-    "ep2d_iterate_f32", "ep2d_track_plastic_zone",
+    "ep2d_iterate_f32", "ep2d_track_plastic_zone", "ep2d_check_grid_barrier",
 )
 
 
@@ -80,6 +80,7 @@ def lib():
         L.ep2d_get_kernel_shape.argtypes = [vp, P(i32), P(i32)]
         L.ep2d_compute_eff_damping.argtypes = [vp, d, P(d), i32, d, P(i64)]
         L.ep2d_polar_fields.argtypes = [vp, d] + [P(d)] * 4 + [P(ctypes.c_uint8)]
+        L.ep2d_check_grid_barrier.argtypes = [i32, i32, i32, i32, i64, P(i32), P(i32)]
         _lib = L
     return _lib
 
@@ -95,6 +96,16 @@ def _dptr(a):
 
 def device_count():
     return int(lib().ep2d_device_count())
+
+
+def check_grid_barrier(blocks, missing=0, rounds=4, timeout_ns=1_000_000, device=0):
+    """The resident form's grid barrier alone (ep2d_check_grid_barrier): `blocks` CTAs
+    meet `rounds` times, `missing` of them never arrive.  Returns (CTAs that passed every
+    round, error flag)."""
+    passed, flag = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().ep2d_check_grid_barrier(int(device), int(blocks), int(missing), int(rounds), int(timeout_ns),
+                                         ctypes.byref(passed), ctypes.byref(flag)))
+    return passed.value, flag.value
 
 
 def make_pa(lx, ly, nx, ny, k0=1.0, g0=0.5, rho0=1.0, cfl=0.5, yield_stress=1.0, porosity=0.005,

@@ -64,9 +64,13 @@ enum {
                              too small to occupy the GPU with strip segments; batches: timed) */
   EP2D_KERNEL_TILE = 1,   /* one CTA per 32-column x `rows`-row tile, stencil halos in
                              shared memory; rows 8, 16 or 32 */
-  EP2D_KERNEL_STREAM = 2  /* one warp per 28-column strip segment of `rows` rows, marching
+  EP2D_KERNEL_STREAM = 2, /* one warp per 28-column strip segment of `rows` rows, marching
                              up its rows with a register window; neighbours by warp
                              shuffles; rows 16 to 1024 */
+  EP2D_KERNEL_RESIDENT = 3 /* the tile form's CTAs kept resident for all the iterations
+                             between two checkpoints: one cooperative launch, a grid-wide
+                             barrier (bounded waits) after each iteration; rows 8, 16 or
+                             32.  Single-RVE handles only (batches refuse it) */
 };
 
 /* pa.dat layout (get_sigma_2D.m:32, read at EffPlast2D.cu:700-707, used at :1563-1573) */
@@ -395,10 +399,21 @@ int ep2d_iterate_f32(ep2d_handle* h, int64_t n_iter);
 /* Iterations this handle has run in the FP32 form of EP2D_F32_BULK (0 for the other
  * precisions).  No counterpart in the reference (all FP64). */
 int ep2d_get_f32_iterations(ep2d_handle* h, int64_t* f32_iterations);
-/* The iteration kernel this handle launches: EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM and
- * its rows per tile / strip segment (the parameters' choice, or the library's).  No
- * counterpart in the reference. */
+/* The iteration kernel this handle launches: EP2D_KERNEL_TILE, EP2D_KERNEL_STREAM or
+ * EP2D_KERNEL_RESIDENT and its rows per tile / strip segment (the parameters' choice, or
+ * the library's).  No counterpart in the reference. */
 int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows);
+/* The resident form's grid barrier on its own, for checking its failure path without a
+ * fault: one cooperative launch of `blocks` CTAs (all resident at once) on `device`
+ * meets at the barrier `rounds` times, except that `missing` of the CTAs never arrive.
+ * With missing == 0 every CTA passes every round (*passed = blocks, *flag = 0); with
+ * missing > 0 the others' waits run out after timeout_ns (at most 10 s) and they return
+ * with the error flag set (*passed = 0, *flag = 1), the context still usable.  A resident
+ * launch whose barrier fails the same way makes the handle's next checkpoint (or the end
+ * of ep2d_iterate / the time step) return EP2D_ERR_CUDA.  No counterpart in the
+ * reference. */
+int ep2d_check_grid_barrier(int32_t device, int32_t blocks, int32_t missing, int32_t rounds, int64_t timeout_ns,
+                            int32_t* passed, int32_t* flag);
 
 #ifdef __cplusplus
 }

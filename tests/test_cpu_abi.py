@@ -91,13 +91,14 @@ def test_solver_without_device_fails_loudly():
     assert e.value.status == _abi.ERR_NODEV
 
 
-@pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "side65537", "field_2e31", "zero_pores", "kernel3",
-                                 "tile_rows12", "stream_rows8", "stream_rows2048", "precision3"])
+@pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "side65537", "field_2e31", "zero_pores", "kernel4",
+                                 "tile_rows12", "stream_rows8", "stream_rows2048", "resident_rows64", "precision3"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
     pa = ep.make_pa(20.0, 20.0, 32, 32)
     nx, nl = 32, 1
-    kw = {"kernel3": dict(kernel=3), "tile_rows12": dict(kernel=ep.KERNEL_TILE, rows=12),
+    kw = {"kernel4": dict(kernel=4), "tile_rows12": dict(kernel=ep.KERNEL_TILE, rows=12),
+          "resident_rows64": dict(kernel=ep.KERNEL_RESIDENT, rows=64),
           "stream_rows8": dict(kernel=ep.KERNEL_STREAM, rows=8),
           "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048),
           "precision3": dict(precision=3)}.get(bad, {})
@@ -134,6 +135,9 @@ def test_batch_and_server_argument_errors():
     with pytest.raises(ep.EP2DError) as e:
         B.batch_solve([s], niter=2000, check_every=1000, rows=12)
     assert e.value.status in (_abi.ERR_ARG, _abi.ERR_NODEV)
+    with pytest.raises(ep.EP2DError) as e:  # the resident form is single-RVE only
+        B.batch_solve([s], niter=2000, check_every=1000, kernel=ep.KERNEL_RESIDENT)
+    assert e.value.status == _abi.ERR_ARG
 
 
 def test_precisions_accepted_by_validation():
@@ -146,6 +150,10 @@ def test_precisions_accepted_by_validation():
         with pytest.raises(ep.EP2DError) as e:
             ep.Solver(32, 32, pa, precision=prec)
         assert e.value.status == _abi.ERR_NODEV, prec
+    for rows in (0, 8, 16, 32):  # so does the resident form with a tile height
+        with pytest.raises(ep.EP2DError) as e:
+            ep.Solver(32, 32, pa, kernel=ep.KERNEL_RESIDENT, rows=rows)
+        assert e.value.status == _abi.ERR_NODEV, rows
 
 
 def test_f32_bulk_footprint_adds_the_perturbation_arrays():

@@ -8,7 +8,8 @@ reference's own CUDA build does); the oracle does not.  Tolerance: every field w
 1e-6).  Both kernel forms are checked: the tile form (CTA per tile, halos in shared
 memory) and the stream form (warp per strip segment, neighbours by shuffles), the
 latter with segments of 16 rows too, so that grids hold several segments, a ragged
-last segment and a ragged last strip.
+last segment and a ragged last strip, and the resident form (the tile form's CTAs kept
+resident across iterations, one cooperative launch per run of plain iterations).
 """
 import numpy as np
 import pytest
@@ -20,8 +21,8 @@ pytestmark = pytest.mark.gpu
 
 FIELDS = ["P", "tauXX", "tauYY", "tauXY", "Ux", "Uy", "Vx", "Vy"]
 PLASTIC_FIELDS = ["tauXYav", "J2", "J2XY"]
-FORMS = [(ep.KERNEL_TILE, 16), (ep.KERNEL_STREAM, 16), (ep.KERNEL_STREAM, 64)]
-FORM_IDS = ["tile16", "stream16", "stream64"]
+FORMS = [(ep.KERNEL_TILE, 16), (ep.KERNEL_STREAM, 16), (ep.KERNEL_STREAM, 64), (ep.KERNEL_RESIDENT, 16)]
+FORM_IDS = ["tile16", "stream16", "stream64", "resident16"]
 
 
 def _pa(n_x, n_y, n_pores=1, porosity=0.01, yield_stress=1.0, g0=0.5):
