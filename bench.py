@@ -778,7 +778,7 @@ def main():
                     help="grid sides of the batched and served objects (the batched workload's distribution "
                          "restricted to these sides so that both fit the default run)")
     ap.add_argument("--extra-niter", type=int, default=1_000_000, help="NITER of the batched and served objects")
-    ap.add_argument("--hbm-iters", type=int, default=2000, help="iterations timed for roofline_hbm")
+    ap.add_argument("--hbm-iters", type=int, default=5000, help="iterations timed for roofline_hbm")
     ap.add_argument("--e2e-solves", type=int, default=1,
                     help="complete converged solves timed end to end through the C ABI (0: skip)")
     args = ap.parse_args()

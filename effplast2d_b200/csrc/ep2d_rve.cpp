@@ -99,10 +99,16 @@ IterShape shape_of(const ep2d_params& p, int sm_count) {
     // faster (256^2: 7 vs 14 us; 512^2: 10 vs 15 us).  Both forms round alike.  Tiles
     // of 8 rows where 16-row tiles would give fewer than two per SM (grids up to ~300^2:
     // 128^2 4.4 vs 5.2 us, 256^2 5.8 vs 7.2 us; 512^2 keeps 16 rows, 10.8 vs 12.1 us).
+    // On elastic RVEs (NL = 1) with at most two 8-row tiles per SM (up to ~256^2) the
+    // resident form, all iterations of a checkpoint interval in one launch, is faster
+    // still (128^2: 4.03 vs 4.39 us, 256^2: 4.55 vs 4.90 us; 320^2: 5.12 vs 4.97); with
+    // the return map (NL > 1) it is slower at every size (256^2: 6.36 vs 5.77 us).
     if (p.kernel == EP2D_KERNEL_AUTO && strips * ((p.ny + SEG_MIN - 1) / SEG_MIN) < 6 * (int64_t)sm_count) {
       s.form = FORM_TILE;
-      const int64_t tiles16 = (int64_t)((p.nx + TILE_X - 1) / TILE_X) * ((p.ny + TILE_Y - 1) / TILE_Y);
+      const int64_t tx = (p.nx + TILE_X - 1) / TILE_X;
+      const int64_t tiles16 = tx * ((p.ny + TILE_Y - 1) / TILE_Y), tiles8 = tx * ((p.ny + 7) / 8);
       s.rows = tiles16 < 2 * (int64_t)sm_count ? 8 : TILE_Y;
+      if (p.nl == 1 && s.rows == 8 && tiles8 <= 2 * (int64_t)sm_count) s.form = FORM_RESIDENT;
     }
   }
   return s;

@@ -61,7 +61,8 @@ enum {
  * operation; they differ in how threads map onto the grid) */
 enum {
   EP2D_KERNEL_AUTO = 0,   /* the library's choice (the stream form; the tile form for grids
-                             too small to occupy the GPU with strip segments; batches: timed) */
+                             too small to occupy the GPU with strip segments, the resident
+                             form for small elastic ones; batches: timed) */
   EP2D_KERNEL_TILE = 1,   /* one CTA per 32-column x `rows`-row tile, stencil halos in
                              shared memory; rows 8, 16 or 32 */
   EP2D_KERNEL_STREAM = 2, /* one warp per 28-column strip segment of `rows` rows, marching
