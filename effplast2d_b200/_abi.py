@@ -139,7 +139,7 @@ class BatchStats(ctypes.Structure):
         ("launches", c_int64), ("all_launches", c_int64), ("cell_updates", c_int64),
         ("rows", c_int32), ("blocks", c_int32),
         ("kernel", c_int32), ("n_tuned", c_int32),
-        ("tune_us", c_double * 6),
+        ("tune_us", c_double * 7),
         ("n_tunes", c_int32), ("solo_intervals", c_int32),
     ]
 

@@ -55,7 +55,7 @@ int validate_config(const ep2d_batch_config& c) {
     sh.form = c.kernel == EP2D_KERNEL_TILE ? FORM_TILE : FORM_STREAM;
     sh.rows = c.rows;
     if (!shape_valid(sh))
-      return fail(EP2D_ERR_ARG, "rows must be 0, or 8, 16 or 32 for the tile form and 16..1024 for the stream form");
+      return fail(EP2D_ERR_ARG, "rows must be 0, or 8, 16 or 32 for the tile form and 4..1024 for the stream form");
   }
   if (c.graph_len < 0 || (c.graph_len % 2) != 0) return fail(EP2D_ERR_ARG, "graph_len must be even");
   return EP2D_OK;
@@ -112,7 +112,7 @@ void BatchEngine::fill_stats(ep2d_batch_stats* st) const {
   st->blocks = blocks;
   st->kernel = shape.form == FORM_TILE ? EP2D_KERNEL_TILE : EP2D_KERNEL_STREAM;
   st->n_tuned = n_tuned;
-  for (int q = 0; q < 6; q++) st->tune_us[q] = tune_us[q];
+  for (int q = 0; q < 7; q++) st->tune_us[q] = tune_us[q];
   st->n_tunes = n_tunes;
   st->solo_intervals = solo_intervals;
 }
@@ -281,14 +281,14 @@ int BatchEngine::launch_plain_run(int64_t k0, int64_t n) {
 }
 
 // Time the candidate kernel shapes (tile form, rows 8/16/32; stream form, rows
-// 32/64/128; only the form cfg.kernel names unless it is AUTO) on real iterations of
+// 8/16/32/64; only the form cfg.kernel names unless it is AUTO) on real iterations of
 // the first interval -- they advance the solution like any other launch -- and keep
 // the fastest.  *k: launches done so far.
 int BatchEngine::autotune(int64_t* k, int64_t n_avail) {
-  IterShape cand[6];
-  int slot[6], nc = 0;
+  IterShape cand[7];
+  int slot[7], nc = 0;
   if (cfg.kernel != EP2D_KERNEL_TILE)
-    for (int q = 0; q < 3; q++) {
+    for (int q = 0; q < 4; q++) {
       cand[nc].form = FORM_STREAM;
       cand[nc].rows = SEG_CHOICES[q];
       slot[nc++] = 3 + q;

@@ -66,7 +66,7 @@ class BatchEngine {
   int n_tuned = 0;   // candidates of the latest tuning run
   int n_tunes = 0;   // tuning runs
   int solo_intervals = 0;  // checkpoint intervals an RVE ran through the single-RVE path
-  double tune_us[6] = {0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 16/32/64
+  double tune_us[7] = {0, 0, 0, 0, 0, 0, 0};  // tile rows 8/16/32, stream rows 8/16/32/64
   void fill_stats(ep2d_batch_stats* st) const;
 
  private:

@@ -80,7 +80,7 @@ int validate_params(const ep2d_params& p) {
   if (p.kernel < EP2D_KERNEL_AUTO || p.kernel > EP2D_KERNEL_RESIDENT) return fail(EP2D_ERR_ARG, "unknown kernel form");
   if (p.rows != 0 && !shape_valid(shape_of(p)))
     return fail(EP2D_ERR_ARG,
-                "rows must be 8, 16 or 32 for the tile and resident forms and 16..1024 for the stream form");
+                "rows must be 8, 16 or 32 for the tile and resident forms and 4..1024 for the stream form");
   return EP2D_OK;
 }
 
@@ -91,24 +91,31 @@ IterShape shape_of(const ep2d_params& p, int sm_count) {
                                               : FORM_STREAM;
   s.rows = p.rows ? p.rows : (s.form == FORM_STREAM ? SEG_DEFAULT : TILE_Y);
   if (p.rows == 0 && s.form == FORM_STREAM && sm_count > 0) {
-    const int64_t strips = (p.nx + STREAM_COLS - 1) / STREAM_COLS;
+    const int64_t strips = (p.nx + STREAM_COLS - 1) / STREAM_COLS, sms = sm_count;
+    auto warps = [&](int rows) { return strips * ((p.ny + rows - 1) / rows); };  // one per segment
+    // Segment height: the tallest power of two from 64 down that gives 16 warps of
+    // segments per SM; below 16 rows the march's three extra rows per segment weigh more
+    // (75 % at 4 rows), so 8 rows stay while they give 9 warps per SM.  Measured, us per
+    // iteration, NL=3: 1024^2 16 rows 16.3 (8: 18.2); 768^2 8 rows 14.3 (16: 16.1);
+    // 640^2 8 rows 9.6 (4: 10.7); 576^2 8 rows 9.6 (4: 9.9); 512^2 4 rows 8.8 (8: 9.5).
     s.rows = 64;
-    while (s.rows > SEG_MIN && strips * ((p.ny + s.rows - 1) / s.rows) < 16 * (int64_t)sm_count) s.rows /= 2;
-    // too few segments to keep 6 warps on every SM (grids up to ~600^2): a warp's march
-    // latency then sets the iteration time, and the tile form, one thread per cell, is
-    // faster (256^2: 7 vs 14 us; 512^2: 10 vs 15 us).  Both forms round alike.  Tiles
-    // of 8 rows where 16-row tiles would give fewer than two per SM (grids up to ~300^2:
-    // 128^2 4.4 vs 5.2 us, 256^2 5.8 vs 7.2 us; 512^2 keeps 16 rows, 10.8 vs 12.1 us).
-    // On elastic RVEs (NL = 1) with at most two 8-row tiles per SM (up to ~256^2) the
-    // resident form, all iterations of a checkpoint interval in one launch, is faster
-    // still (128^2: 4.03 vs 4.39 us, 256^2: 4.55 vs 4.90 us; 320^2: 5.12 vs 4.97); with
-    // the return map (NL > 1) it is slower at every size (256^2: 6.36 vs 5.77 us).
-    if (p.kernel == EP2D_KERNEL_AUTO && strips * ((p.ny + SEG_MIN - 1) / SEG_MIN) < 6 * (int64_t)sm_count) {
+    while (s.rows > SEG_MIN && warps(s.rows) < (s.rows > 8 ? 16 : 9) * sms) s.rows /= 2;
+    // Too few 4-row segments to keep the SMs busy: a warp's march latency then sets the
+    // iteration time, and the tile form, one thread per cell, is faster.  With the
+    // return map (NL > 1) below 5.5 warps per SM (256^2: tile 5.8 vs 4-row stream 6.1 us;
+    // 320^2: 6.5 vs 6.1), elastic RVEs below 12 (384^2: 5.6 vs 6.0; 512^2: 6.9 vs 6.2).
+    // Both forms round alike.  Tiles of 8 rows where 16-row tiles would give fewer than
+    // two per SM (128^2 4.4 vs 5.2 us, 256^2 5.8 vs 7.2 us).  On elastic RVEs with at
+    // most two 8-row tiles per SM (up to ~256^2) the resident form, all iterations of a
+    // checkpoint interval in one launch, is faster still (128^2: 4.03 vs 4.39 us, 256^2:
+    // 4.55 vs 4.90 us; 320^2: 5.12 vs 4.97); with the return map it is slower at every
+    // size (256^2: 6.36 vs 5.77 us).
+    if (p.kernel == EP2D_KERNEL_AUTO && 2 * warps(SEG_MIN) < (p.nl == 1 ? 24 : 11) * sms) {
       s.form = FORM_TILE;
       const int64_t tx = (p.nx + TILE_X - 1) / TILE_X;
       const int64_t tiles16 = tx * ((p.ny + TILE_Y - 1) / TILE_Y), tiles8 = tx * ((p.ny + 7) / 8);
-      s.rows = tiles16 < 2 * (int64_t)sm_count ? 8 : TILE_Y;
-      if (p.nl == 1 && s.rows == 8 && tiles8 <= 2 * (int64_t)sm_count) s.form = FORM_RESIDENT;
+      s.rows = tiles16 < 2 * sms ? 8 : TILE_Y;
+      if (p.nl == 1 && s.rows == 8 && tiles8 <= 2 * sms) s.form = FORM_RESIDENT;
     }
   }
   return s;

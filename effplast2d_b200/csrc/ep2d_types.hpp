@@ -70,9 +70,9 @@ constexpr int TILE_Y_CHOICES[3] = {8, 16, 32};
 // launches).
 enum IterForm { FORM_TILE = 0, FORM_STREAM = 1, FORM_RESIDENT = 2 };
 constexpr int STREAM_COLS = 28;  // columns a warp of the stream form owns (32 lanes, 2-lane halos)
-constexpr int SEG_MIN = 16, SEG_MAX = 1024;
+constexpr int SEG_MIN = 4, SEG_MAX = 1024;
 constexpr int SEG_DEFAULT = 64;
-constexpr int SEG_CHOICES[3] = {16, 32, 64};  // the batch autotuner's stream-form candidates
+constexpr int SEG_CHOICES[4] = {8, 16, 32, 64};  // the batch autotuner's stream-form candidates
 struct IterShape {
   int form = FORM_STREAM;
   int rows = SEG_DEFAULT;

@@ -60,14 +60,15 @@ enum {
 /* form of the fused iteration kernel (both compute the same iteration, operation for
  * operation; they differ in how threads map onto the grid) */
 enum {
-  EP2D_KERNEL_AUTO = 0,   /* the library's choice (the stream form; the tile form for grids
-                             too small to occupy the GPU with strip segments, the resident
-                             form for small elastic ones; batches: timed) */
+  EP2D_KERNEL_AUTO = 0,   /* the library's choice (the stream form, segments of 4 to 64
+                             rows by grid size; the tile form for grids too small to occupy
+                             the GPU even with 4-row segments, the resident form for small
+                             elastic ones; batches: timed) */
   EP2D_KERNEL_TILE = 1,   /* one CTA per 32-column x `rows`-row tile, stencil halos in
                              shared memory; rows 8, 16 or 32 */
   EP2D_KERNEL_STREAM = 2, /* one warp per 28-column strip segment of `rows` rows, marching
                              up its rows with a register window; neighbours by warp
-                             shuffles; rows 16 to 1024 */
+                             shuffles; rows 4 to 1024 */
   EP2D_KERNEL_RESIDENT = 3 /* the tile form's CTAs kept resident for all the iterations
                              between two checkpoints: one cooperative launch, a grid-wide
                              barrier (bounded waits) after each iteration; rows 8, 16 or
@@ -179,7 +180,7 @@ typedef struct ep2d_batch_config {
   int32_t precision;      /* EP2D_FP64 or EP2D_MIXED (FP32 velocity storage) */
   int32_t device;
   int32_t rows;           /* rows per tile (tile form: 8, 16, 32) or strip segment (stream
-                             form: 16..1024); 0 = pick form and rows by timing the first
+                             form: 4..1024); 0 = pick form and rows by timing the first
                              launches of the batch */
   int32_t graph_len;      /* iterations per captured CUDA graph (even; 0 = 64) */
   int32_t kernel;         /* EP2D_KERNEL_*; with rows != 0, AUTO means the stream form */
@@ -195,8 +196,8 @@ typedef struct ep2d_batch_stats {
   int32_t blocks;         /* persistent grid size (CTAs) */
   int32_t kernel;         /* EP2D_KERNEL_TILE or EP2D_KERNEL_STREAM: the form used */
   int32_t n_tuned;        /* candidates timed by the latest autotuning run */
-  double tune_us[6];      /* measured us per launch in the latest autotuning run: tile form
-                             rows 8, 16, 32, stream form rows 16, 32, 64 (0 if untimed) */
+  double tune_us[7];      /* measured us per launch in the latest autotuning run: tile form
+                             rows 8, 16, 32, stream form rows 8, 16, 32, 64 (0 if untimed) */
   int32_t n_tunes;        /* autotuning runs: one when the batch starts, and one whenever
                              the set of active RVEs has changed at a checkpoint */
   int32_t solo_intervals; /* RVE checkpoint intervals run through the single-RVE path (its

@@ -92,14 +92,14 @@ def test_solver_without_device_fails_loudly():
 
 
 @pytest.mark.parametrize("bad", ["nan_dx", "nl65", "nl0", "tiny", "side65537", "field_2e31", "zero_pores", "kernel4",
-                                 "tile_rows12", "stream_rows8", "stream_rows2048", "resident_rows64", "precision3"])
+                                 "tile_rows12", "stream_rows2", "stream_rows2048", "resident_rows64", "precision3"])
 def test_invalid_params_rejected_before_device(bad):
     # argument validation runs before any device call, so it is testable without a GPU
     pa = ep.make_pa(20.0, 20.0, 32, 32)
     nx, nl = 32, 1
     kw = {"kernel4": dict(kernel=4), "tile_rows12": dict(kernel=ep.KERNEL_TILE, rows=12),
           "resident_rows64": dict(kernel=ep.KERNEL_RESIDENT, rows=64),
-          "stream_rows8": dict(kernel=ep.KERNEL_STREAM, rows=8),
+          "stream_rows2": dict(kernel=ep.KERNEL_STREAM, rows=2),
           "stream_rows2048": dict(kernel=ep.KERNEL_STREAM, rows=2048),
           "precision3": dict(precision=3)}.get(bad, {})
     if bad == "nan_dx":

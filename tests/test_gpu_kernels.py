@@ -133,7 +133,7 @@ def test_homogeneous_affine_is_equilibrium():
 
 
 @pytest.mark.parametrize("grid", [(301, 203), (242, 130)], ids=["301x203", "242x130"])
-@pytest.mark.parametrize("rows", [16, 64, 256])
+@pytest.mark.parametrize("rows", [4, 8, 12, 16, 64, 256])
 def test_stream_form_matches_tile_form(rows, grid):
     # Both forms evaluate the same explicitly rounded per-cell formulas, so they agree
     # bit for bit.  The grids are wider and taller than several strips and segments,
