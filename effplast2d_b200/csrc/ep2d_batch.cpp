@@ -378,13 +378,15 @@ int BatchEngine::advance(Slot& s, double error) {
 }
 
 // True if the RVE keeps the GPU busy alone: its own kernel shape (shape_of) is the stream
-// form with 16 warps' worth of strip segments on every SM.  Such an RVE gains nothing
-// from sharing launches with others and runs its iterations through the single-RVE path
-// (its own shape, overlapped launches, its own captured graphs); smaller ones share the
-// batched launches.
+// form with segments of 16 rows or more and 16 warps' worth of them on every SM.  Such
+// an RVE gains nothing from sharing launches with others and runs its iterations through
+// the single-RVE path (its own shape, overlapped launches, its own captured graphs);
+// smaller ones share the batched launches.  Shorter segments are the single-RVE path's
+// answer to a grid too small to fill the GPU (768^2 alone: 8-row segments, 41 G
+// cell-updates/s), which a shared launch beats.
 bool BatchEngine::fills_gpu(const Rve& r) const {
   const IterShape sh = shape_of(r.prm, sm_count_);
-  if (sh.form != FORM_STREAM) return false;
+  if (sh.form != FORM_STREAM || sh.rows < 16) return false;
   int ux = 0, uy = 0;
   shape_units(sh, r.g.nx, r.g.ny, &ux, &uy);
   return (int64_t)ux * uy >= 16 * (int64_t)sm_count_;
