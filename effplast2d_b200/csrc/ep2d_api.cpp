@@ -248,6 +248,7 @@ int ep2d_check_grid_barrier(int32_t device, int32_t blocks, int32_t missing, int
   if (blocks < 1 || missing < 0 || missing > blocks || rounds < 0 || timeout_ns < 0)
     return fail(EP2D_ERR_ARG, "need 1 <= blocks, 0 <= missing <= blocks, rounds >= 0, timeout_ns >= 0");
   if (timeout_ns > 10000000000LL) return fail(EP2D_ERR_ARG, "timeout_ns above 10 s");
+  if (rounds > 1000000) return fail(EP2D_ERR_ARG, "rounds above 1,000,000");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EP2D_ERR_NODEV, "no CUDA device");
   if (device < 0 || device >= ndev) return fail(EP2D_ERR_ARG, "device index out of range");

@@ -407,7 +407,8 @@ int ep2d_get_f32_iterations(ep2d_handle* h, int64_t* f32_iterations);
 int ep2d_get_kernel_shape(ep2d_handle* h, int32_t* kernel, int32_t* rows);
 /* The resident form's grid barrier on its own, for checking its failure path without a
  * fault: one cooperative launch of `blocks` CTAs (all resident at once) on `device`
- * meets at the barrier `rounds` times, except that `missing` of the CTAs never arrive.
+ * meets at the barrier `rounds` times (at most 1,000,000), except that `missing` of the
+ * CTAs never arrive.
  * With missing == 0 every CTA passes every round (*passed = blocks, *flag = 0); with
  * missing > 0 the others' waits run out after timeout_ns (at most 10 s) and they return
  * with the error flag set (*passed = 0, *flag = 1), the context still usable.  A resident

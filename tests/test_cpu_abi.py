@@ -164,3 +164,12 @@ def test_f32_bulk_footprint_adds_the_perturbation_arrays():
     # four float arrays of the common pitch (96 for nx = 64) x 65 rows, 256-byte aligned
     extra = 4 * (((96 * 65 * 4) + 255) // 256 * 256)
     assert B.footprint(s, ep.F32_BULK) == B.footprint(s) + extra
+
+
+def test_grid_barrier_check_arguments_before_device():
+    # the barrier check validates its arguments before any device call
+    for kw in (dict(blocks=0), dict(blocks=4, missing=5), dict(blocks=4, rounds=-1),
+               dict(blocks=4, rounds=2_000_000), dict(blocks=4, timeout_ns=20_000_000_000)):
+        with pytest.raises(ep.EP2DError) as e:
+            ep.check_grid_barrier(**kw)
+        assert e.value.status == _abi.ERR_ARG, kw

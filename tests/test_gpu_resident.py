@@ -113,7 +113,7 @@ def test_grid_barrier_wait_runs_out_and_context_survives():
 
 def test_barrier_check_arguments():
     for kw in (dict(blocks=0), dict(blocks=4, missing=5), dict(blocks=4, rounds=-1),
-               dict(blocks=4, timeout_ns=20_000_000_000)):
+               dict(blocks=4, rounds=2_000_000), dict(blocks=4, timeout_ns=20_000_000_000)):
         with pytest.raises(ep.EP2DError) as e:
             ep.check_grid_barrier(**kw)
         assert e.value.status == ep.ERR_ARG
